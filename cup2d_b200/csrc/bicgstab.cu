@@ -1,0 +1,773 @@
+// BiCGSTAB with the 64x64 block-Jacobi preconditioner, one persistent launch
+// per solve.
+//
+//   k_bicgstab64     plain FP64: the drop-in form of BiCGSTABSolver::main
+//                    (source/Poisson/BiCGSTAB.cu:412-620)
+//   k_bicgstab_mixed FP32 Krylov vectors and split-TF32 tensor-core P^-1;
+//                    FP64 solution update, FP64 true-residual replacement
+//                    ("reliable updates") and FP64 convergence test
+//
+// The reference runs each iteration as ~25 library launches (cuSPARSE COO
+// SpMV, cuBLAS dot/nrm2/axpy/scal/Idamax/Dgemm), 8 one-thread scalar kernels
+// and 4 host round-trips.  Here one cooperative kernel runs the whole solve.
+// Each CTA owns a contiguous range of blocks; an iteration is five fused
+// passes over them, separated by bounded grid barriers:
+//
+//   A  p = r + beta (p - omega nu);  z = P^-1 p          (R r,p,nu  W p,z)
+//   B  nu = A z;  (rhat, nu)                             (R z,rhat  W nu)
+//   C  x += alpha z;  s = r - alpha nu;  z = P^-1 s      (R x,z,r,nu W x,r,z)
+//   D  t = A z;  (t,s), (t,t)                            (R z,s     W t)
+//   E  x += omega z;  r = s - omega t;  |r|_inf, (rhat,r), |r|^2, |rhat|^2
+//                                                        (R x,z,s,t,rhat W x,r)
+//
+// Scalar recurrences, the breakdown/restart rule (rho^2 < 1e-16|r|^2|rhat|^2),
+// best-iterate tracking and the L-inf stopping test follow the reference.
+// Every CTA reduces the per-CTA partials in the same fixed order (FP64), so
+// all CTAs take identical decisions and results are bitwise reproducible for
+// a given grid.  The best iterate is copied lazily: pass C of the next
+// iteration stores the old x when the previous iterate was the best so far.
+//
+// Mixed form.  A correction accumulated in FP32 loses eps32*kappa of the
+// residual (kappa ~ 1e5..1e7 on these meshes), so restarted FP32 inner
+// solves cannot refine.  Instead x stays FP64 and is updated in passes C and
+// E from the FP32 z; only the Krylov vectors (r, rhat, p, nu, t, z) are
+// FP32.  When the FP32 residual has dropped by `reliable_delta` since its
+// last replacement, or claims convergence, it is replaced by the true
+// residual b - A x computed in FP64 (with b projected to zero sum, the
+// Neumann compatibility condition), without restarting the recurrences.
+// Convergence is declared only on the true FP64 residual.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.hpp"
+#include "spmv.cuh"
+
+namespace cup2d {
+
+namespace {
+
+constexpr int kWarps = kSolveThreads / 32;
+constexpr int kPad = 68;  // staged block row (conflict-free fragment loads)
+
+enum : int {
+  Q_INIT = 0,   // 3: |A x0|_inf, |r0|_inf, |r0|^2
+  Q_RHNU = 3,   // pass B
+  Q_TS = 4,     // pass D: (t,s), (t,t)
+  Q_RMAX = 6,   // pass E: |r|_inf, (rhat,r), |r|^2, |rhat|^2
+  Q_HX = 10,    // mean removal: sum h^2 x, sum h^2
+  Q_RU = 12,    // true residual: |r64|_inf, (rhat,r), |r|^2, |rhat|^2, |r32|_inf
+  Q_SUMB = 17   // sum b
+};
+static_assert(Q_SUMB + 1 <= kRedQ, "reduction slots");
+
+struct Smem {
+  union {
+    double d[2][8][kPad];
+    float f[2][16][kPad];
+  } tile;
+  double wred[kWarps][6];
+  double gres[6];
+  int flag;
+};
+
+// max that propagates NaN (fmax drops it, which would let a blown-up
+// residual read as converged)
+__device__ __forceinline__ double nanmax(double a, double b) { return (a > b || a != a) ? a : b; }
+
+template <int NV>
+__device__ __forceinline__ void cta_partials(Smem& sm, const double (&v)[NV], unsigned is_max,
+                                             double* __restrict__ red, int q0) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double r = v[q];
+    if ((is_max >> q) & 1u) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r = nanmax(r, __shfl_xor_sync(kFull, r, o));
+    } else {
+      r = warp_sum(r);
+    }
+    if (lane == 0) sm.wred[w][q] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    const int q = threadIdx.x;
+    double acc = sm.wred[0][q];
+    for (int k = 1; k < kWarps; ++k)
+      acc = ((is_max >> q) & 1u) ? nanmax(acc, sm.wred[k][q]) : acc + sm.wred[k][q];
+    red[(q0 + q) * gridDim.x + blockIdx.x] = acc;
+  }
+}
+
+template <int NV>
+__device__ __forceinline__ void grid_reduce(Smem& sm, unsigned is_max, const double* __restrict__ red, int q0) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (w < NV) {
+    const bool mx = (is_max >> w) & 1u;
+    const double* src = red + (q0 + w) * gridDim.x;
+    double acc = 0.0;
+    for (unsigned j = lane; j < gridDim.x; j += 32) {
+      const double v = __ldcg(src + j);
+      acc = mx ? nanmax(acc, v) : acc + v;
+    }
+    if (mx) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc = nanmax(acc, __shfl_xor_sync(kFull, acc, o));
+    } else {
+      acc = warp_sum(acc);
+    }
+    if (lane == 0) sm.gres[w] = acc;
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------ P^-1 tile application ----
+
+template <class T>
+struct Pinv;
+
+// FP64: tiles of 8 blocks; warp w computes rows 8w..8w+7 with DMMA m8n8k4,
+// P^-1 fragments (16 per lane) in registers for the whole solve.
+template <>
+struct Pinv<double> {
+  static constexpr int kTile = 8;
+  double af[16];
+  __device__ __forceinline__ void load(const double* __restrict__ P, const float*, int w, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) af[kk] = __ldg(P + (8 * w + g) * kBLEN + 4 * kk + t);
+  }
+  __device__ __forceinline__ static double (*rows(Smem& sm, int buf))[kPad] { return sm.tile.d[buf]; }
+  __device__ __forceinline__ void apply(const double (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
+                                        double* __restrict__ z) const {
+    const int g = lane >> 2, t = lane & 3;
+    double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 16; kk += 2) {
+      dmma_884(c0, c1, af[kk], tile[g][4 * kk + t]);
+      dmma_884(e0, e1, af[kk + 1], tile[g][4 * (kk + 1) + t]);
+    }
+    c0 += e0;
+    c1 += e1;
+    if (2 * t < nvalid) z[(tb + 2 * t) * kBLEN + 8 * w + g] = c0;
+    if (2 * t + 1 < nvalid) z[(tb + 2 * t + 1) * kBLEN + 8 * w + g] = c1;
+  }
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// FP32: tiles of 16 blocks; warp w computes rows 16*(w&3).. of blocks
+// 8*(w>>2).. with m16n8k8 TF32 MMA.  Operands are split x = hi + lo (both
+// TF32) and z = Phi*hi + Phi*lo + Plo*hi, accumulated in FP32, which keeps
+// the preconditioner apply at FP32 accuracy.
+template <>
+struct Pinv<float> {
+  static constexpr int kTile = 16;
+  uint32_t ahi[8][4], alo[8][4];
+  __device__ __forceinline__ void load(const double*, const float* __restrict__ P32, int w, int lane) {
+    const int g = lane >> 2, t = lane & 3, m = w & 3;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const float v[4] = {__ldg(P32 + (16 * m + g) * kBLEN + 8 * kk + t),
+                          __ldg(P32 + (16 * m + g + 8) * kBLEN + 8 * kk + t),
+                          __ldg(P32 + (16 * m + g) * kBLEN + 8 * kk + t + 4),
+                          __ldg(P32 + (16 * m + g + 8) * kBLEN + 8 * kk + t + 4)};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        ahi[kk][q] = to_tf32(v[q]);
+        alo[kk][q] = to_tf32(v[q] - __uint_as_float(ahi[kk][q]));
+      }
+    }
+  }
+  __device__ __forceinline__ static float (*rows(Smem& sm, int buf))[kPad] { return sm.tile.f[buf]; }
+  __device__ __forceinline__ void apply(const float (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
+                                        float* __restrict__ z) const {
+    const int g = lane >> 2, t = lane & 3, m = w & 3, nt = w >> 2;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const float* brow = tile[8 * nt + g];
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const float x0 = brow[8 * kk + t], x1 = brow[8 * kk + t + 4];
+      const uint32_t h0 = to_tf32(x0), h1 = to_tf32(x1);
+      const uint32_t l0 = to_tf32(x0 - __uint_as_float(h0)), l1 = to_tf32(x1 - __uint_as_float(h1));
+      mma_tf32(acc, alo[kk], h0, h1);
+      mma_tf32(acc, ahi[kk], l0, l1);
+      mma_tf32(acc, ahi[kk], h0, h1);
+    }
+    const int n0 = 8 * nt + 2 * t, n1 = n0 + 1;
+    const int r0 = 16 * m + g, r1 = r0 + 8;
+    if (n0 < nvalid) {
+      z[(tb + n0) * kBLEN + r0] = acc[0];
+      z[(tb + n0) * kBLEN + r1] = acc[2];
+    }
+    if (n1 < nvalid) {
+      z[(tb + n1) * kBLEN + r0] = acc[1];
+      z[(tb + n1) * kBLEN + r1] = acc[3];
+    }
+  }
+};
+
+// ----------------------------------------------------- iteration core -----
+
+template <class T, class X>
+struct Vecs {
+  X* x;   // iterate
+  X* xo;  // best iterate (lazy copy)
+  T* r;   // residual; s in place between passes C and E
+  T* rh;
+  T* p;
+  T* nu;
+  T* t;
+  T* z;
+};
+
+struct IterState {
+  double rho, nr, nrh;  // (rhat,r), |r|^2, |rhat|^2 of the current residual
+  double err_init;      // L-inf norm the relative test divides by
+  double err_opt;       // best residual norm seen (recursive)
+  double err_true;      // mixed: last true residual |b - A x|_inf
+  int restarts;
+  int iters;
+  int updates;          // mixed: true-residual replacements
+  int status;
+  bool best_is_x;
+};
+
+__device__ __forceinline__ double dprod(double a, double b) { return a * b; }
+__device__ __forceinline__ double dprod(float a, float b) { return (double)a * (double)b; }
+
+// Mixed form: r = (b - mean_b) - A x in FP64, stored as FP32 (and as rhat
+// when set_rh); partials |r64|_inf, (rhat,r), |r|^2, |rhat|^2, |r32|_inf.
+__device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
+                                              double mean_b, const double* __restrict__ x, float* __restrict__ r,
+                                              float* __restrict__ rh, bool set_rh, double* __restrict__ red,
+                                              int64_t b0, int64_t b1) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+    const int64_t o = blk * kBLEN;
+    const double x0 = __ldcg(x + o + lane), x1 = __ldcg(x + o + lane + 32);
+    double y[2];
+    spmv_block<double>(M, blk, x, lane, x0, x1, y[0], y[1]);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t i = o + lane + 32 * h;
+      const double r64 = (__ldg(b + i) - mean_b) - y[h];
+      const float r32 = (float)r64;
+      r[i] = r32;
+      float rhv;
+      if (set_rh) {
+        rh[i] = r32;
+        rhv = r32;
+      } else {
+        rhv = __ldcg(rh + i);
+      }
+      v[0] = nanmax(v[0], fabs(r64));
+      v[1] += dprod(rhv, r32);
+      v[2] += dprod(r32, r32);
+      v[3] += dprod(rhv, rhv);
+      v[4] = nanmax(v[4], fabs((double)r32));
+    }
+  }
+  cta_partials<5>(sm, v, 0x11u, red, Q_RU);
+}
+
+struct MixedCtx {  // what the reliable update needs
+  const double* b;
+  double mean_b;
+  double delta;
+  double tol_abs, tol_rel;
+  bool restart;  // restart the recurrences at each replacement
+};
+
+// Runs BiCGSTABSolver::main's loop from a prepared state (r, rhat = r,
+// st.rho/nr/nrh/err_init set, p = nu = 0 implied).  T is the Krylov type,
+// X the solution type; RU enables the mixed form's true-residual
+// replacement.  Returns false if a barrier gave up.
+template <class T, class X, bool RU>
+__device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const Pinv<T>& pin,
+                              const Vecs<T, X> V, double* __restrict__ red, int64_t b0, int64_t b1,
+                              double tol_abs, double tol_rel, int max_restarts, int max_iter, const MixedCtx& mx,
+                              IterState& st) {
+  constexpr int TB = Pinv<T>::kTile;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const double eps = 1e-21;
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0, beta;
+  bool zero_pnu = true;
+  double rho = st.rho, nr = st.nr, nrh = st.nrh;
+  double rmax_since = sqrt(nr);  // largest |r|_2 since the last true residual
+  int k;
+  st.status = CUP2D_NOT_CONVERGED;
+  for (k = 0; k < max_iter; ++k) {
+    // scalar step (BiCGSTAB.cu:471-509)
+    const bool serious_breakdown = rho * rho < 1e-16 * nr * nrh;
+    beta = (rho / (rho_prev + eps)) * (alpha / (omega + eps));
+    bool restart_now = false;
+    if (serious_breakdown && max_restarts > 0) {
+      ++st.restarts;
+      if (st.restarts >= max_restarts) { st.status = CUP2D_BREAKDOWN_LIMIT; break; }
+      restart_now = true;
+      rho = nr;  // |rhat|^2 after rhat = r
+      nrh = nr;
+      zero_pnu = true;
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0;
+      beta = (rho / (rho_prev + eps)) * (alpha / (omega + eps));
+    }
+    const T tb_beta = (T)beta, tb_omega = (T)omega;
+    // pass A: p = r + beta (p - omega nu); z = P^-1 p
+    {
+      int buf = 0;
+      for (int64_t tb = b0; tb < b1; tb += TB) {
+        const int nvalid = (int)imin64(TB, b1 - tb);
+        auto tile = Pinv<T>::rows(sm, buf);
+        for (int j = w; j < TB; j += kWarps) {
+          if (j < nvalid) {
+            const int64_t o = (tb + j) * kBLEN;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int64_t i = o + lane + 32 * h;
+              const T rv = __ldcg(V.r + i);
+              T pv;
+              if (zero_pnu) pv = rv;
+              else pv = rv + tb_beta * (__ldcg(V.p + i) - tb_omega * __ldcg(V.nu + i));
+              if (restart_now) V.rh[i] = rv;
+              V.p[i] = pv;
+              tile[j][lane + 32 * h] = pv;
+            }
+          } else {
+            tile[j][lane] = T(0);
+            tile[j][lane + 32] = T(0);
+          }
+        }
+        __syncthreads();
+        pin.apply(tile, w, lane, tb, nvalid, V.z);
+        buf ^= 1;
+      }
+      zero_pnu = false;
+    }
+    if (!B.sync(&sm.flag)) return false;
+    // pass B: nu = A z; (rhat, nu)
+    {
+      double v[1] = {0.0};
+      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+        const int64_t o = blk * kBLEN;
+        const T z0 = __ldcg(V.z + o + lane), z1 = __ldcg(V.z + o + lane + 32);
+        T y0, y1;
+        spmv_block<T>(M, blk, V.z, lane, z0, z1, y0, y1);
+        V.nu[o + lane] = y0;
+        V.nu[o + lane + 32] = y1;
+        v[0] += dprod(__ldcg(V.rh + o + lane), y0) + dprod(__ldcg(V.rh + o + lane + 32), y1);
+      }
+      cta_partials<1>(sm, v, 0u, red, Q_RHNU);
+    }
+    if (!B.sync(&sm.flag)) return false;
+    grid_reduce<1>(sm, 0u, red, Q_RHNU);
+    alpha = rho / (sm.gres[0] + eps);
+    const T ta = (T)alpha;
+    // pass C: x += alpha z; s = r - alpha nu; z = P^-1 s
+    {
+      int buf = 0;
+      for (int64_t tb = b0; tb < b1; tb += TB) {
+        const int nvalid = (int)imin64(TB, b1 - tb);
+        auto tile = Pinv<T>::rows(sm, buf);
+        for (int j = w; j < TB; j += kWarps) {
+          if (j < nvalid) {
+            const int64_t o = (tb + j) * kBLEN;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int64_t i = o + lane + 32 * h;
+              const X xv = __ldcg(V.x + i);
+              if (st.best_is_x) V.xo[i] = xv;
+              V.x[i] = xv + (X)alpha * (X)__ldcg(V.z + i);
+              const T sv = __ldcg(V.r + i) - ta * __ldcg(V.nu + i);
+              V.r[i] = sv;
+              tile[j][lane + 32 * h] = sv;
+            }
+          } else {
+            tile[j][lane] = T(0);
+            tile[j][lane + 32] = T(0);
+          }
+        }
+        __syncthreads();
+        pin.apply(tile, w, lane, tb, nvalid, V.z);
+        buf ^= 1;
+      }
+    }
+    if (!B.sync(&sm.flag)) return false;
+    // pass D: t = A z; (t,s), (t,t)
+    {
+      double v[2] = {0.0, 0.0};
+      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+        const int64_t o = blk * kBLEN;
+        const T z0 = __ldcg(V.z + o + lane), z1 = __ldcg(V.z + o + lane + 32);
+        T y0, y1;
+        spmv_block<T>(M, blk, V.z, lane, z0, z1, y0, y1);
+        V.t[o + lane] = y0;
+        V.t[o + lane + 32] = y1;
+        v[0] += dprod(y0, __ldcg(V.r + o + lane)) + dprod(y1, __ldcg(V.r + o + lane + 32));
+        v[1] += dprod(y0, y0) + dprod(y1, y1);
+      }
+      cta_partials<2>(sm, v, 0u, red, Q_TS);
+    }
+    if (!B.sync(&sm.flag)) return false;
+    grid_reduce<2>(sm, 0u, red, Q_TS);
+    omega = sm.gres[0] / (sm.gres[1] + eps);
+    const T to = (T)omega;
+    // pass E: x += omega z; r = s - omega t; norms
+    {
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+        const int64_t o = blk * kBLEN;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t i = o + lane + 32 * h;
+          V.x[i] = __ldcg(V.x + i) + (X)omega * (X)__ldcg(V.z + i);
+          const T rn = __ldcg(V.r + i) - to * __ldcg(V.t + i);
+          V.r[i] = rn;
+          const T rhv = __ldcg(V.rh + i);
+          v[0] = nanmax(v[0], fabs((double)rn));
+          v[1] += dprod(rhv, rn);
+          v[2] += dprod(rn, rn);
+          v[3] += dprod(rhv, rhv);
+        }
+      }
+      cta_partials<4>(sm, v, 0x1u, red, Q_RMAX);
+    }
+    if (!B.sync(&sm.flag)) return false;
+    grid_reduce<4>(sm, 0x1u, red, Q_RMAX);
+    double error = sm.gres[0];
+    double rho_new = sm.gres[1];
+    nr = sm.gres[2];
+    nrh = sm.gres[3];
+    if (!(error == error) || !(rho_new == rho_new)) {  // non-finite: stop, keep the best iterate
+      st.best_is_x = false;
+      ++k;
+      break;
+    }
+    bool refreshed = false;
+    if constexpr (RU) {
+      rmax_since = fmax(rmax_since, sqrt(nr));
+      const bool claims = (error <= tol_abs) || (error / st.err_init <= tol_rel);
+      if (claims || sqrt(nr) < mx.delta * rmax_since) {
+        // pass E's barrier already ordered every CTA's x update before this
+        true_residual(sm, M, mx.b, mx.mean_b, V.x, V.r, V.rh, mx.restart, red, b0, b1);
+        if (!B.sync(&sm.flag)) return false;
+        grid_reduce<5>(sm, 0x11u, red, Q_RU);
+        ++st.updates;
+        refreshed = true;
+        st.err_true = sm.gres[0];
+        rho_new = sm.gres[1];
+        nr = sm.gres[2];
+        nrh = sm.gres[3];
+        error = sm.gres[4];
+        rmax_since = sqrt(nr);
+        if ((st.err_true <= mx.tol_abs) || (st.err_true / st.err_init <= mx.tol_rel)) {
+          st.err_opt = fmin(st.err_opt, error);
+          st.best_is_x = true;
+          st.status = CUP2D_OK;
+          ++k;
+          break;
+        }
+      }
+    }
+    // convergence (BiCGSTAB.cu:571-600)
+    if (error < st.err_opt) {
+      st.err_opt = error;
+      st.best_is_x = true;
+      if (!RU && ((error <= tol_abs) || (error / st.err_init <= tol_rel))) {
+        st.status = CUP2D_OK;
+        ++k;
+        break;
+      }
+    } else {
+      st.best_is_x = false;
+    }
+    if (RU && refreshed && mx.restart) {
+      // rhat = r was written with the true residual: fresh recurrences
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0;
+      rho = rho_new;
+      zero_pnu = true;
+    } else {
+      rho_prev = rho;
+      rho = rho_new;
+    }
+  }
+  st.iters += k;
+  return true;
+}
+
+// x -= sum(h^2 x)/sum(h^2) over the CTA's blocks (ExpAMRSolver.cpp:383-415);
+// x already holds the final iterate.
+__device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, double* __restrict__ x,
+                              double* __restrict__ red, int64_t b0, int64_t b1) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double v[2] = {0.0, 0.0};
+  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+    const int64_t o = blk * kBLEN;
+    const double hb = __ldg(M.hblk + blk);
+    v[0] += (__ldcg(x + o + lane) + __ldcg(x + o + lane + 32)) * (hb * hb);
+    v[1] += 2.0 * (hb * hb);
+  }
+  cta_partials<2>(sm, v, 0u, red, Q_HX);
+  if (!B.sync(&sm.flag)) return false;
+  grid_reduce<2>(sm, 0u, red, Q_HX);
+  const double avg = sm.gres[0] / sm.gres[1];
+  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+    const int64_t o = blk * kBLEN;
+    x[o + lane] = __ldcg(x + o + lane) - avg;
+    x[o + lane + 32] = __ldcg(x + o + lane + 32) - avg;
+  }
+  return true;
+}
+
+// x <- x_opt when the last iterate was not the best
+__device__ __forceinline__ void take_best(bool best_is_x, double* __restrict__ x, const double* __restrict__ xo,
+                                          int64_t b0, int64_t b1) {
+  if (best_is_x) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+    const int64_t o = blk * kBLEN;
+    x[o + lane] = __ldcg(xo + o + lane);
+    x[o + lane + 32] = __ldcg(xo + o + lane + 32);
+  }
+}
+
+}  // namespace
+
+// ====================================================== plain FP64 ========
+
+__global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab64(SolveArgs64 S) {
+  __shared__ Smem sm;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t nb = S.M.nb;
+  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u};
+  Pinv<double> pin;
+  pin.load(S.P, nullptr, w, lane);
+  const MeshView& M = S.M;
+  const Vecs<double, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
+
+  // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
+  {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+      const int64_t o = blk * kBLEN;
+      const double x0 = __ldcg(S.x + o + lane), x1 = __ldcg(S.x + o + lane + 32);
+      double y0, y1;
+      spmv_block<double>(M, blk, S.x, lane, x0, x1, y0, y1);
+      const double r0 = __ldg(S.b + o + lane) - y0, r1 = __ldg(S.b + o + lane + 32) - y1;
+      S.r[o + lane] = r0; S.r[o + lane + 32] = r1;
+      S.rh[o + lane] = r0; S.rh[o + lane + 32] = r1;
+      v[0] = nanmax(v[0], nanmax(fabs(y0), fabs(y1)));
+      v[1] = nanmax(v[1], nanmax(fabs(r0), fabs(r1)));
+      v[2] += r0 * r0 + r1 * r1;
+    }
+    cta_partials<3>(sm, v, 0x3u, S.red, Q_INIT);
+  }
+  if (!B.sync(&sm.flag)) return;
+  grid_reduce<3>(sm, 0x3u, S.red, Q_INIT);
+  IterState st;
+  const double norm_ax0 = sm.gres[0];
+  st.err_init = sm.gres[1];
+  st.err_opt = st.err_init;
+  st.err_true = st.err_init;
+  st.rho = st.nr = st.nrh = sm.gres[2];
+  st.restarts = 0;
+  st.iters = 0;
+  st.updates = 0;
+  st.best_is_x = true;
+  st.status = CUP2D_NOT_CONVERGED;
+  const MixedCtx none{};
+  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, S.red, b0, b1, S.tol_abs, S.tol_rel,
+                                            S.max_restarts, S.max_iter, none, st))
+    return;
+  take_best(st.best_is_x, S.x, S.xo, b0, b1);
+  if (S.subtract_mean && !subtract_mean(sm, B, M, S.x, S.red, b0, b1)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.stats->status = st.status;
+    S.stats->iterations = st.iters;
+    S.stats->restarts = st.restarts;
+    S.stats->refinements = 0;
+    S.stats->err_init = st.err_init;
+    S.stats->err_opt = st.err_opt;
+    S.stats->norm_ax0 = norm_ax0;
+  }
+}
+
+// ================================================ mixed precision =========
+
+__global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab_mixed(SolveArgsMixed S) {
+  __shared__ Smem sm;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t nb = S.M.nb;
+  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u};
+  Pinv<float> pin;
+  pin.load(nullptr, S.P32, w, lane);
+  const Vecs<float, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
+
+  // Neumann compatibility: project b to zero sum (sum b / n)
+  {
+    double v[1] = {0.0};
+    for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
+      const int64_t o = blk * kBLEN;
+      v[0] += __ldg(S.b + o + lane) + __ldg(S.b + o + lane + 32);
+    }
+    cta_partials<1>(sm, v, 0u, S.red, Q_SUMB);
+  }
+  if (!B.sync(&sm.flag)) return;
+  grid_reduce<1>(sm, 0u, S.red, Q_SUMB);
+  MixedCtx mx;
+  mx.b = S.b;
+  mx.mean_b = sm.gres[0] / (double)(nb * kBLEN);
+  mx.delta = S.reliable_delta;
+  mx.tol_abs = S.tol_abs;
+  mx.tol_rel = S.tol_rel;
+  mx.restart = S.reliable_restart != 0;
+  true_residual(sm, S.M, S.b, mx.mean_b, S.x, S.r, S.rh, true, S.red, b0, b1);
+  if (!B.sync(&sm.flag)) return;
+  grid_reduce<5>(sm, 0x11u, S.red, Q_RU);
+  IterState st;
+  st.err_init = sm.gres[0];
+  st.err_true = sm.gres[0];
+  st.err_opt = sm.gres[4];
+  st.rho = sm.gres[1];
+  st.nr = sm.gres[2];
+  st.nrh = sm.gres[3];
+  st.restarts = 0;
+  st.iters = 0;
+  st.updates = 0;
+  st.best_is_x = true;
+  st.status = CUP2D_NOT_CONVERGED;
+  const bool done0 = st.err_true <= S.tol_abs || st.err_true == 0.0;
+  if (done0) {
+    st.status = CUP2D_OK;
+  } else if (!bicgstab_loop<float, double, true>(sm, B, S.M, pin, V, S.red, b0, b1, S.tol_abs, S.tol_rel,
+                                                 S.max_restarts, S.max_iter, mx, st)) {
+    return;
+  }
+  take_best(st.best_is_x, S.x, S.xo, b0, b1);
+  if (S.subtract_mean && !subtract_mean(sm, B, S.M, S.x, S.red, b0, b1)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.stats->status = st.status;
+    S.stats->iterations = st.iters;
+    S.stats->restarts = st.restarts;
+    S.stats->refinements = st.updates;
+    S.stats->err_init = st.err_init;
+    S.stats->err_opt = st.status == CUP2D_OK ? st.err_true : st.err_opt;
+    S.stats->norm_ax0 = 0.0;
+  }
+}
+
+// ------------------------------------------------------------ launch -----
+
+namespace {
+int coop_grid(const void* fn, int device) {
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolveThreads, 0) != cudaSuccess) return 0;
+  return sms * per_sm;
+}
+}  // namespace
+
+int max_coop_grid_fp64(int device) { return coop_grid((const void*)k_bicgstab64, device); }
+int max_coop_grid_mixed(int device) { return coop_grid((const void*)k_bicgstab_mixed, device); }
+
+cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s) {
+  void* args[] = {const_cast<SolveArgs64*>(&a)};
+  return cudaLaunchCooperativeKernel((const void*)k_bicgstab64, dim3(grid), dim3(kSolveThreads), args, 0, s);
+}
+
+cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s) {
+  void* args[] = {const_cast<SolveArgsMixed*>(&a)};
+  return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args, 0, s);
+}
+
+// ------------------------------------------------------- single ops -------
+
+__global__ void __launch_bounds__(256) k_spmv64(MeshView M, const double* __restrict__ x, double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t blk = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); blk < M.nb; blk += warps) {
+    const int64_t o = blk * kBLEN;
+    const double x0 = x[o + lane], x1 = x[o + lane + 32];
+    double y0, y1;
+    spmv_block<double>(M, blk, x, lane, x0, x1, y0, y1);
+    y[o + lane] = y0;
+    y[o + lane + 32] = y1;
+  }
+}
+
+cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s) {
+  if (M.nb <= 0) return cudaSuccess;
+  const int64_t ctas = (M.nb + 7) / 8;
+  k_spmv64<<<(unsigned)(ctas < 65535 ? ctas : 65535), 256, 0, s>>>(M, x, y);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int64_t nb,
+                                                             const double* __restrict__ p, double* __restrict__ z) {
+  __shared__ double tile[8][kPad];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Pinv<double> pin;
+  pin.load(P, nullptr, w, lane);
+  for (int64_t tb = (int64_t)blockIdx.x * 8; tb < nb; tb += (int64_t)gridDim.x * 8) {
+    const int nvalid = (int)imin64(8, nb - tb);
+    if (w < nvalid) {
+      tile[w][lane] = p[(tb + w) * kBLEN + lane];
+      tile[w][lane + 32] = p[(tb + w) * kBLEN + lane + 32];
+    } else {
+      tile[w][lane] = 0.0;
+      tile[w][lane + 32] = 0.0;
+    }
+    __syncthreads();
+    pin.apply(tile, w, lane, tb, nvalid, z);
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s) {
+  if (nb <= 0) return cudaSuccess;
+  const int64_t ctas = (nb + 7) / 8;
+  k_precond64<<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(P, nb, p, z);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __restrict__ P32, int64_t nb,
+                                                             const float* __restrict__ p, float* __restrict__ z) {
+  __shared__ float tile[16][kPad];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Pinv<float> pin;
+  pin.load(nullptr, P32, w, lane);
+  for (int64_t tb = (int64_t)blockIdx.x * 16; tb < nb; tb += (int64_t)gridDim.x * 16) {
+    const int nvalid = (int)imin64(16, nb - tb);
+    for (int j = w; j < 16; j += kWarps) {
+      tile[j][lane] = j < nvalid ? p[(tb + j) * kBLEN + lane] : 0.f;
+      tile[j][lane + 32] = j < nvalid ? p[(tb + j) * kBLEN + lane + 32] : 0.f;
+    }
+    __syncthreads();
+    pin.apply(tile, w, lane, tb, nvalid, z);
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s) {
+  if (nb <= 0) return cudaSuccess;
+  const int64_t ctas = (nb + 15) / 16;
+  k_precond32<<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(P32, nb, p, z);
+  return cudaGetLastError();
+}
+
+}  // namespace cup2d

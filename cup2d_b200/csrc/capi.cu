@@ -1,0 +1,564 @@
+// C ABI of the B200 Poisson solver (include/cup2d_poisson.h).
+//
+// A handle plays the roles of ExpAMRSolver + LocalSpMatDnVec + BiCGSTABSolver
+// in CUP2D (source/Poisson/ExpAMRSolver.cpp, LocalSpMatDnVec.cpp, BiCGSTAB.cu):
+// it owns P^-1, the assembled operator and the Krylov vectors on the device.
+// Unlike BiCGSTABSolver::updateAll (BiCGSTAB.cu:142-244), a mesh update
+// reuses its buffers when the new mesh fits and assembles on the device; a
+// solve is one persistent kernel launch and one 64-byte status read.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "../../include/cup2d_poisson.h"
+#include "forest.hpp"
+#include "kernels.hpp"
+
+using namespace cup2d;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  int64_t cap = 0;  // elements
+  int ensure(int64_t n) {
+    if (n <= cap && p) return CUP2D_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const int64_t m = std::max<int64_t>(n, 1);
+    if (cudaMalloc(&p, sizeof(T) * m) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return CUP2D_OOM;
+    }
+    cap = m;
+    return CUP2D_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+int validate_opts(const cup2d_solve_opts& o) {
+  if (!(o.tol_abs >= 0.0) || !(o.tol_rel >= 0.0)) return CUP2D_INVALID_ARGUMENT;
+  if (o.max_iter < 0 || o.max_restarts < 0) return CUP2D_INVALID_ARGUMENT;
+  if (!(o.reliable_delta > 0.0 && o.reliable_delta < 1.0)) return CUP2D_INVALID_ARGUMENT;
+  if (o.reliable_restart != 0 && o.reliable_restart != 1) return CUP2D_INVALID_ARGUMENT;
+  if (o.precision != CUP2D_PREC_FP64 && o.precision != CUP2D_PREC_MIXED) return CUP2D_INVALID_ARGUMENT;
+  if (o.timeout_ms <= 0) return CUP2D_INVALID_ARGUMENT;
+  return CUP2D_OK;
+}
+
+int from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return CUP2D_OK;
+  if (e == cudaErrorMemoryAllocation) return CUP2D_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return CUP2D_NO_DEVICE;
+  return CUP2D_CUDA_ERROR;
+}
+
+}  // namespace
+
+struct cup2d_poisson {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cup2d_solve_opts opts{};
+  // forest
+  int32_t bpdx = 0, bpdy = 0, level_max = 0, px = 0, py = 0;
+  double extent = 1.0;
+  int64_t nb = 0;
+  // operator
+  DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol;
+  DevBuf<unsigned long long> xmask;
+  DevBuf<double> hblk, xval, P;
+  DevBuf<float> xval32, P32;
+  DevBuf<int> err;
+  DeviceMesh mesh;
+  // Krylov vectors (FP64)
+  DevBuf<double> xo, r, rh, p, nu, t, z, bstage, xstage;
+  // mixed-precision vectors
+  DevBuf<float> f_r, f_rh, f_p, f_nu, f_t, f_z;
+  // persistent-kernel scratch
+  DevBuf<double> red;
+  DevBuf<unsigned> bar;
+  DevBuf<int> abort_flag;
+  DevBuf<DevStats> dstats;
+  DevStats* hstats = nullptr;  // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int grid64 = 0, gridmx = 0;      // max co-resident grids
+  int grid_override = 0;           // tuner / user choice (0 = heuristic)
+  int blocks_per_cta = 8;          // heuristic target
+
+  int grid_for(int maxg) const {
+    if (grid_override > 0) return std::min(grid_override, maxg);
+    const int64_t want = (nb + blocks_per_cta - 1) / blocks_per_cta;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, maxg));
+  }
+};
+
+namespace {
+
+int alloc_rows_cb(void* ctx, int64_t R) {
+  auto* h = static_cast<cup2d_poisson*>(ctx);
+  int st = h->rowlen.ensure(R);
+  if (st) return st;
+  st = h->xptr.ensure(R + 1);
+  if (st) return st;
+  h->mesh.rowlen = h->rowlen.p;
+  h->mesh.xptr = h->xptr.p;
+  return CUP2D_OK;
+}
+
+int alloc_nnz_cb(void* ctx, int64_t nnz) {
+  auto* h = static_cast<cup2d_poisson*>(ctx);
+  int st = h->xcol.ensure(nnz);
+  if (st) return st;
+  st = h->xval.ensure(nnz);
+  if (st) return st;
+  st = h->xval32.ensure(nnz);
+  if (st) return st;
+  h->mesh.xcol = h->xcol.p;
+  h->mesh.xval = h->xval.p;
+  h->mesh.xval32 = h->xval32.p;
+  return CUP2D_OK;
+}
+
+int check_forest(const cup2d_forest* f) {
+  if (!f || f->nblocks <= 0 || !f->level || !f->bx || !f->by) return CUP2D_INVALID_ARGUMENT;
+  if (f->bpdx < 1 || f->bpdy < 1 || f->level_max < 1 || f->level_max > kMaxLevels || !(f->extent > 0.0))
+    return CUP2D_INVALID_ARGUMENT;
+  if (f->nblocks > (int64_t)(INT32_MAX / kBLEN)) return CUP2D_INVALID_ARGUMENT;
+  const int64_t entries = leaf_table_entries(f->bpdx, f->bpdy, f->level_max);
+  if (entries > ((int64_t)1 << 30)) return CUP2D_BAD_MESH;  // dense tables would exceed 4 GB
+  return CUP2D_OK;
+}
+
+int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
+  int st = check_forest(f);
+  if (st) return st;
+  const int64_t nb = f->nblocks, n = nb * kBLEN;
+  const int64_t entries = leaf_table_entries(f->bpdx, f->bpdy, f->level_max);
+  if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb)) ||
+      (st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
+      (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
+      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
+    return st;
+  // Krylov vectors
+  if ((st = h->xo.ensure(n)) || (st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) ||
+      (st = h->nu.ensure(n)) || (st = h->t.ensure(n)) || (st = h->z.ensure(n)))
+    return st;
+  cudaStream_t s = h->stream;
+  if (cudaMemcpyAsync(h->level.p, f->level, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(h->bx.p, f->bx, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(h->by.p, f->by, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  DeviceMesh& m = h->mesh;
+  m.nb = nb;
+  m.level = h->level.p;
+  m.bx = h->bx.p;
+  m.by = h->by.p;
+  m.table = h->table.p;
+  m.nbr = h->nbr.p;
+  m.xmask = h->xmask.p;
+  m.xcount = h->xcount.p;
+  m.xbase = h->xbase.p;
+  m.hblk = h->hblk.p;
+  m.scan_tmp = h->scan_tmp.p;
+  m.err = h->err.p;
+  m.ctx = h;
+  m.alloc_rows = alloc_rows_cb;
+  m.alloc_nnz = alloc_nnz_cb;
+  // a mesh without explicit rows still needs valid (empty) row arrays
+  if ((st = alloc_rows_cb(h, 0)) || (st = alloc_nnz_cb(h, 0))) return st;
+  AssembleIn in{f->bpdx, f->bpdy, f->level_max, f->periodic_x, f->periodic_y, nb,
+                f->extent / ((double)std::max(f->bpdx, f->bpdy) * 8.0)};
+  st = assemble_on_device(in, m, s);
+  if (st) return st;
+  h->bpdx = f->bpdx;
+  h->bpdy = f->bpdy;
+  h->level_max = f->level_max;
+  h->px = f->periodic_x;
+  h->py = f->periodic_y;
+  h->extent = f->extent;
+  h->nb = nb;
+  return CUP2D_OK;
+}
+
+int ensure_scratch(cup2d_poisson* h) {
+  int st;
+  const int g = std::max(h->grid64, h->gridmx);
+  if ((st = h->red.ensure((int64_t)kRedQ * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
+      (st = h->abort_flag.ensure(1)) || (st = h->dstats.ensure(1)))
+    return st;
+  return CUP2D_OK;
+}
+
+int ensure_mixed(cup2d_poisson* h) {
+  const int64_t n = h->nb * kBLEN;
+  int st;
+  if ((st = h->f_r.ensure(n)) || (st = h->f_rh.ensure(n)) || (st = h->f_p.ensure(n)) ||
+      (st = h->f_nu.ensure(n)) || (st = h->f_t.ensure(n)) || (st = h->f_z.ensure(n)))
+    return st;
+  return CUP2D_OK;
+}
+
+void fill_stats(const cup2d_poisson* h, int launch_status, float ms, cup2d_solve_stats* out) {
+  const DevStats& d = *h->hstats;
+  out->status = launch_status != CUP2D_OK ? launch_status : d.status;
+  out->iterations = d.iterations;
+  out->restarts = d.restarts;
+  out->refinements = d.refinements;
+  out->err_init = d.err_init;
+  out->err_final = d.err_opt;
+  out->rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
+  out->solve_ms = ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cup2d_version(void) { return "cup2d_b200 0.1.0 (sm_100a)"; }
+
+const char* cup2d_status_string(int s) {
+  switch (s) {
+    case CUP2D_OK: return "ok";
+    case CUP2D_NOT_CONVERGED: return "not converged (iteration cap)";
+    case CUP2D_BREAKDOWN_LIMIT: return "restart cap reached after breakdowns";
+    case CUP2D_BAD_MESH: return "invalid forest (overlap, hole or 2:1 violation)";
+    case CUP2D_OOM: return "device allocation failed";
+    case CUP2D_TIMEOUT: return "device-side wait timed out";
+    case CUP2D_CUDA_ERROR: return "CUDA error";
+    case CUP2D_INVALID_ARGUMENT: return "invalid argument";
+    case CUP2D_NO_DEVICE: return "no CUDA device";
+    case CUP2D_QUEUE_FULL: return "queue full";
+    case CUP2D_PENDING: return "pending";
+    default: return "unknown status";
+  }
+}
+
+void cup2d_default_opts(cup2d_solve_opts* o) {
+  if (!o) return;
+  o->tol_abs = 0.0;
+  o->tol_rel = 1e-8;
+  o->max_restarts = 100;
+  o->max_iter = 1000;
+  o->precision = CUP2D_PREC_FP64;
+  o->subtract_mean = 1;
+  o->reliable_delta = 0.1;
+  o->reliable_restart = 1;
+  o->timeout_ms = 20000;
+}
+
+int cup2d_pinv(double* P_out) {
+  if (!P_out) return CUP2D_INVALID_ARGUMENT;
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * 4096) != cudaSuccess) return CUP2D_OOM;
+  cudaError_t e = launch_build_pinv(d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(P_out, d, sizeof(double) * 4096, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return from_cuda(e);
+}
+
+int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cup2d_poisson** out) {
+  if (!out) return CUP2D_INVALID_ARGUMENT;
+  *out = nullptr;
+  cup2d_solve_opts o;
+  cup2d_default_opts(&o);
+  if (opts) o = *opts;
+  int st = validate_opts(o);
+  if (st) return st;
+  if ((st = check_forest(forest))) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CUP2D_NO_DEVICE;
+  }
+  auto* h = new (std::nothrow) cup2d_poisson();
+  if (!h) return CUP2D_OOM;
+  h->opts = o;
+  cudaGetDevice(&h->device);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+      cudaMallocHost(&h->hstats, sizeof(DevStats)) != cudaSuccess) {
+    cup2d_poisson_destroy(h);
+    return CUP2D_CUDA_ERROR;
+  }
+  h->grid64 = max_coop_grid_fp64(h->device);
+  h->gridmx = max_coop_grid_mixed(h->device);
+  if (h->grid64 <= 0 || h->gridmx <= 0) {
+    cup2d_poisson_destroy(h);
+    return CUP2D_CUDA_ERROR;
+  }
+  if (const char* e = std::getenv("CUP2D_GRID")) h->grid_override = std::atoi(e);
+  if ((st = h->P.ensure(4096)) || (st = h->P32.ensure(4096)) || (st = ensure_scratch(h))) {
+    cup2d_poisson_destroy(h);
+    return st;
+  }
+  cudaError_t e = launch_build_pinv(h->P.p, h->stream);
+  if (e == cudaSuccess) e = launch_convert_f64_f32(h->P.p, h->P32.p, 4096, h->stream);
+  if (e != cudaSuccess) {
+    cup2d_poisson_destroy(h);
+    return from_cuda(e);
+  }
+  if ((st = do_assemble(h, forest))) {
+    cup2d_poisson_destroy(h);
+    return st;
+  }
+  *out = h;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest) {
+  if (!h) return CUP2D_INVALID_ARGUMENT;
+  return do_assemble(h, forest);
+}
+
+int cup2d_poisson_set_opts(cup2d_poisson* h, const cup2d_solve_opts* opts) {
+  if (!h || !opts) return CUP2D_INVALID_ARGUMENT;
+  int st = validate_opts(*opts);
+  if (st) return st;
+  h->opts = *opts;
+  return CUP2D_OK;
+}
+
+int64_t cup2d_poisson_num_cells(const cup2d_poisson* h) { return h ? h->nb * kBLEN : 0; }
+
+int cup2d_poisson_set_grid(cup2d_poisson* h, int32_t grid) {
+  if (!h || grid < 0) return CUP2D_INVALID_ARGUMENT;
+  h->grid_override = grid;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_destroy(cup2d_poisson* h) {
+  if (!h) return CUP2D_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  DevBuf<int32_t>* i32[] = {&h->level, &h->bx, &h->by, &h->table, &h->nbr, &h->xcount, &h->xbase,
+                            &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol};
+  for (auto* b : i32) b->release();
+  h->xmask.release();
+  DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
+                           &h->z, &h->bstage, &h->xstage, &h->red};
+  for (auto* b : f64) b->release();
+  DevBuf<float>* f32[] = {&h->xval32, &h->P32, &h->f_r, &h->f_rh, &h->f_p,
+                          &h->f_nu, &h->f_t, &h->f_z};
+  for (auto* b : f32) b->release();
+  h->err.release();
+  h->bar.release();
+  h->abort_flag.release();
+  h->dstats.release();
+  if (h->hstats) cudaFreeHost(h->hstats);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x, cup2d_solve_stats* stats,
+                               void* stream) {
+  if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  const cup2d_solve_opts& o = h->opts;
+  int st;
+  if ((st = ensure_scratch(h))) return st;
+  if (cudaMemsetAsync(h->bar.p, 0, sizeof(unsigned), s) != cudaSuccess ||
+      cudaMemsetAsync(h->abort_flag.p, 0, sizeof(int), s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  const unsigned long long tns = (unsigned long long)o.timeout_ms * 1000000ull;
+  // the barrier counter counts arrivals of the whole solve in 32 bits
+  const int grid = o.precision == CUP2D_PREC_MIXED ? h->grid_for(h->gridmx) : h->grid_for(h->grid64);
+  const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
+  if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
+  if (stats) cudaEventRecord(h->ev0, s);
+  cudaError_t e;
+  if (o.precision == CUP2D_PREC_MIXED) {
+    if ((st = ensure_mixed(h))) return st;
+    SolveArgsMixed a{};
+    a.M = h->mesh.view();
+    a.P32 = h->P32.p;
+    a.b = d_b;
+    a.x = d_x;
+    a.xo = h->xo.p;
+    a.r = h->f_r.p;
+    a.rh = h->f_rh.p;
+    a.p = h->f_p.p;
+    a.nu = h->f_nu.p;
+    a.t = h->f_t.p;
+    a.z = h->f_z.p;
+    a.red = h->red.p;
+    a.bar = h->bar.p;
+    a.abort_flag = h->abort_flag.p;
+    a.stats = h->dstats.p;
+    a.tol_abs = o.tol_abs;
+    a.tol_rel = o.tol_rel;
+    a.reliable_delta = o.reliable_delta;
+    a.reliable_restart = o.reliable_restart;
+    a.max_restarts = o.max_restarts;
+    a.max_iter = o.max_iter;
+    a.subtract_mean = o.subtract_mean;
+    a.timeout_ns = tns;
+    e = launch_bicgstab_mixed(a, grid, s);
+  } else {
+    SolveArgs64 a{};
+    a.M = h->mesh.view();
+    a.P = h->P.p;
+    a.b = d_b;
+    a.x = d_x;
+    a.xo = h->xo.p;
+    a.r = h->r.p;
+    a.rh = h->rh.p;
+    a.p = h->p.p;
+    a.nu = h->nu.p;
+    a.t = h->t.p;
+    a.z = h->z.p;
+    a.red = h->red.p;
+    a.bar = h->bar.p;
+    a.abort_flag = h->abort_flag.p;
+    a.stats = h->dstats.p;
+    a.tol_abs = o.tol_abs;
+    a.tol_rel = o.tol_rel;
+    a.max_restarts = o.max_restarts;
+    a.max_iter = o.max_iter;
+    a.subtract_mean = o.subtract_mean;
+    a.timeout_ns = tns;
+    e = launch_bicgstab64(a, grid, s);
+  }
+  if (e != cudaSuccess) return from_cuda(e);
+  if (!stats) return CUP2D_OK;
+  int habort = 0;
+  cudaEventRecord(h->ev1, s);
+  if (cudaMemcpyAsync(h->hstats, h->dstats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&habort, h->abort_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  fill_stats(h, habort ? CUP2D_TIMEOUT : CUP2D_OK, ms, stats);
+  return stats->status == CUP2D_TIMEOUT ? CUP2D_TIMEOUT : CUP2D_OK;
+}
+
+int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x, cup2d_solve_stats* stats) {
+  if (!h || !b || !x) return CUP2D_INVALID_ARGUMENT;
+  const int64_t n = h->nb * kBLEN;
+  int st;
+  if ((st = h->bstage.ensure(n)) || (st = h->xstage.ensure(n))) return st;
+  cudaStream_t s = h->stream;
+  if (cudaMemcpyAsync(h->bstage.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(h->xstage.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  cup2d_solve_stats local;
+  st = cup2d_poisson_solve_device(h, h->bstage.p, h->xstage.p, stats ? stats : &local, s);
+  if (st != CUP2D_OK && st != CUP2D_NOT_CONVERGED && st != CUP2D_BREAKDOWN_LIMIT) return st;
+  if (cudaMemcpyAsync(x, h->xstage.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream) {
+  if (!h || !d_x || !d_y) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, s));
+}
+
+int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream) {
+  if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  return from_cuda(launch_precond64(h->P.p, h->nb, d_p, d_z, s));
+}
+
+int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream) {
+  if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  return from_cuda(launch_precond32(h->P32.p, h->nb, d_p, d_z, s));
+}
+
+int cup2d_poisson_explicit_info(cup2d_poisson* h, int64_t* rows, int64_t* nnz) {
+  if (!h) return CUP2D_INVALID_ARGUMENT;
+  if (rows) *rows = h->mesh.R;
+  if (nnz) *nnz = h->mesh.nnz;
+  return CUP2D_OK;
+}
+
+// Expands the block-structured operator into the CSR that getMat would
+// produce: interior rows as (iy-1, ix-1, self, ix+1, iy+1) with (1,1,-4,1,1);
+// implicit edge rows in getMat's face order through an ordered map; explicit
+// rows verbatim.
+int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n_out, int64_t* nnz_out, int64_t* row_ptr,
+                             int32_t* col, double* val) {
+  if (!h) return CUP2D_INVALID_ARGUMENT;
+  const int64_t nb = h->nb, n = nb * kBLEN;
+  std::vector<int32_t> nbr(4 * nb), xbase(nb + 1), xptr(h->mesh.R + 1), xcol(h->mesh.nnz);
+  std::vector<unsigned long long> xmask(nb);
+  std::vector<double> xval(h->mesh.nnz);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  if (cudaMemcpy(nbr.data(), h->nbr.p, 4 * nb * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xbase.data(), h->xbase.p, (nb + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xmask.data(), h->xmask.p, nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xptr.data(), h->xptr.p, (h->mesh.R + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  if (h->mesh.nnz > 0 &&
+      (cudaMemcpy(xcol.data(), h->xcol.p, h->mesh.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+       cudaMemcpy(xval.data(), h->xval.p, h->mesh.nnz * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+    return CUP2D_CUDA_ERROR;
+  int64_t nnz = 0;
+  const bool fill = row_ptr && col && val;
+  if (fill) row_ptr[0] = 0;
+  for (int64_t b = 0; b < nb; ++b)
+    for (int c = 0; c < kBLEN; ++c) {
+      const int ix = c & 7, iy = c >> 3;
+      const int64_t self = b * kBLEN + c;
+      auto push = [&](int64_t cc, double v) {
+        if (fill) {
+          col[nnz] = (int32_t)cc;
+          val[nnz] = v;
+        }
+        ++nnz;
+      };
+      if (ix > 0 && ix < 7 && iy > 0 && iy < 7) {
+        push(self - 8, 1);
+        push(self - 1, 1);
+        push(self, -4);
+        push(self + 1, 1);
+        push(self + 8, 1);
+      } else if ((xmask[b] >> c) & 1ull) {
+        const int r = xbase[b] + __builtin_popcountll(xmask[b] & ((1ull << c) - 1ull));
+        for (int k = xptr[r]; k < xptr[r + 1]; ++k) push(xcol[k], xval[k]);
+      } else {
+        std::map<int64_t, double> row;
+        const bool valid[4] = {ix > 0, ix < 7, iy > 0, iy < 7};
+        const int64_t inb[4] = {self - 1, self + 1, self - 8, self + 8};
+        for (int f = 0; f < 4; ++f) {
+          int64_t nc = -1;
+          if (valid[f]) {
+            nc = inb[f];
+          } else if (nbr[4 * b + f] >= 0) {
+            const int64_t o = (int64_t)nbr[4 * b + f] * kBLEN;
+            nc = f == 0 ? o + iy * 8 + 7 : f == 1 ? o + iy * 8 : f == 2 ? o + 56 + ix : o + ix;
+          } else {
+            continue;  // wall
+          }
+          row[nc] += 1.0;
+          row[self] += -1.0;
+        }
+        for (auto& kv : row) push(kv.first, kv.second);
+      }
+      if (fill) row_ptr[self + 1] = nnz;
+    }
+  if (n_out) *n_out = n;
+  if (nnz_out) *nnz_out = nnz;
+  return CUP2D_OK;
+}
+
+}  // extern "C"

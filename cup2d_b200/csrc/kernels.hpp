@@ -1,0 +1,138 @@
+// Host-side launch interface of the device kernels (internal to the library).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace cup2d {
+
+constexpr int kMaxLevels = 24;
+
+struct AssembleIn {
+  int32_t bpdx, bpdy, level_max, periodic_x, periodic_y;
+  int64_t nblocks;
+  double h0;  // cell size at level 0
+};
+
+// Device buffers of one assembled operator.  Buffers sized by the block
+// count are allocated by the owner before assembly; the explicit-row
+// buffers are allocated through the callbacks once their sizes are known.
+struct DeviceMesh {
+  int64_t nb = 0;
+  int32_t* level = nullptr;
+  int32_t* bx = nullptr;
+  int32_t* by = nullptr;
+  int32_t* table = nullptr;       // per-level dense leaf tables
+  int32_t* nbr = nullptr;         // [4*nb]
+  unsigned long long* xmask = nullptr;  // [nb]
+  int32_t* xcount = nullptr;      // [nb]
+  int32_t* xbase = nullptr;       // [nb+1]
+  double* hblk = nullptr;         // [nb]
+  int32_t* scan_tmp = nullptr;
+  int* err = nullptr;
+  int64_t R = 0, nnz = 0;
+  int32_t* rowlen = nullptr;      // [R]
+  int32_t* xptr = nullptr;        // [R+1]
+  int32_t* xcol = nullptr;        // [nnz]
+  double* xval = nullptr;         // [nnz]
+  float* xval32 = nullptr;        // [nnz]
+  void* ctx = nullptr;
+  int (*alloc_rows)(void* ctx, int64_t R) = nullptr;
+  int (*alloc_nnz)(void* ctx, int64_t nnz) = nullptr;
+
+  MeshView view() const {
+    MeshView v;
+    v.nb = nb;
+    v.nbr = nbr;
+    v.xmask = xmask;
+    v.xbase = xbase;
+    v.xptr = xptr;
+    v.xcol = xcol;
+    v.xval = xval;
+    v.xval32 = xval32;
+    v.hblk = hblk;
+    return v;
+  }
+};
+
+int64_t leaf_table_entries(int bpdx, int bpdy, int level_max);
+int64_t scan_temp_ints(int64_t n);
+int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s);
+cudaError_t launch_build_pinv(double* d_P, cudaStream_t s);
+cudaError_t launch_convert_f64_f32(const double* a, float* b, int64_t n, cudaStream_t s);
+cudaError_t launch_exclusive_scan(const int32_t* in, int64_t n, int32_t* out, int32_t* tmp, cudaStream_t s);
+
+// ------------------------------------------------------------ solver ----
+
+// Per-solve results written by the persistent kernel (one struct per solve).
+struct DevStats {
+  int status;        // cup2d_status
+  int iterations;
+  int restarts;
+  int refinements;
+  double err_init;
+  double err_opt;
+  double norm_ax0;
+  double pad;
+};
+
+constexpr int kRedQ = 20;  // reduction quantities per CTA
+
+struct SolveArgs64 {
+  MeshView M;
+  const double* P;      // 64x64 row-major
+  const double* b;
+  double* x;            // x0 in, solution out
+  double* xo;           // best iterate (lazy copy)
+  double* r;            // r, and s in place
+  double* rh;
+  double* p;
+  double* nu;
+  double* t;
+  double* z;
+  double* red;          // [kRedQ][grid]
+  unsigned* bar;        // arrival counter, zeroed before launch
+  int* abort_flag;      // zeroed before launch
+  DevStats* stats;
+  double tol_abs, tol_rel;
+  int max_restarts, max_iter, subtract_mean;
+  unsigned long long timeout_ns;
+};
+
+// Mixed precision: FP32 Krylov vectors, FP64 solution and true residual.
+struct SolveArgsMixed {
+  MeshView M;
+  const float* P32;     // 64x64 row-major FP32 P^-1 (rounded from the FP64 build)
+  const double* b;
+  double* x;            // FP64 solution (in/out), updated every iteration
+  double* xo;           // FP64 best iterate (lazy copy)
+  float* r;
+  float* rh;
+  float* p;
+  float* nu;
+  float* t;
+  float* z;
+  double* red;
+  unsigned* bar;
+  int* abort_flag;
+  DevStats* stats;
+  double tol_abs, tol_rel, reliable_delta;
+  int max_restarts, max_iter, subtract_mean, reliable_restart;
+  unsigned long long timeout_ns;
+};
+
+constexpr int kSolveThreads = 256;
+
+// Largest co-resident grid of the persistent kernels on this device.
+int max_coop_grid_fp64(int device);
+int max_coop_grid_mixed(int device);
+cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s);
+cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s);
+
+// Single operations (tests, residual checks).
+cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s);
+cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s);
+cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s);
+
+}  // namespace cup2d

@@ -1,0 +1,250 @@
+"""Python mirror of CUP2D's Poisson-solver interface on the B200 C ABI.
+
+Reference interface (paths in the CUP2D tree):
+  class PoissonSolver { virtual void solve(const ScalarGrid* input,
+                                           ScalarGrid* output) = 0; }   source/Poisson/Base.h:8-13
+  makePoissonSolver(SimulationData&)                                    source/Poisson/Base.cpp:8-30
+  libcubismup2d.poisson.Solver.solve(input, output)                     source/Bindings/Poisson.cpp:10-11
+  ExpAMRSolver::solve (tolerances, re-assembly, mean removal)           source/Poisson/ExpAMRSolver.cpp:354-416
+
+`ScalarGrid` here is a mesh plus one value per cell, (nblocks, 8, 8) in
+block order (numpy on the host, or a CUDA tensor).  `Solver` is the handle
+level API: solves on host arrays or device tensors, plus the building
+blocks (operator apply, preconditioner, assembled CSR) used by the tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from .mesh import Mesh
+
+
+def _pd(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def default_opts() -> L.SolveOpts:
+    o = L.SolveOpts()
+    L.lib().cup2d_default_opts(C.byref(o))
+    return o
+
+
+def make_opts(tol_abs=0.0, tol_rel=1e-8, max_restarts=100, max_iter=1000, precision="fp64",
+              subtract_mean=True, reliable_delta=0.1, reliable_restart=True, timeout_ms=20000) -> L.SolveOpts:
+    o = default_opts()
+    o.tol_abs = tol_abs
+    o.tol_rel = tol_rel
+    o.max_restarts = max_restarts
+    o.max_iter = max_iter
+    o.precision = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision] if isinstance(precision, str) \
+        else int(precision)
+    o.subtract_mean = int(bool(subtract_mean))
+    o.reliable_delta = reliable_delta
+    o.reliable_restart = int(bool(reliable_restart))
+    o.timeout_ms = timeout_ms
+    return o
+
+
+class Solver:
+    """One solver handle: P^-1 and the assembled operator resident on the GPU."""
+
+    def __init__(self, mesh: Mesh, opts: Optional[L.SolveOpts] = None, **kw):
+        self.mesh = mesh
+        self.opts = opts if opts is not None else make_opts(**kw)
+        self._h = C.c_void_p()
+        f = mesh.forest()
+        L.check(L.lib().cup2d_poisson_create(C.byref(f), C.byref(self.opts), C.byref(self._h)),
+                "cup2d_poisson_create")
+        self.last_stats: Optional[dict] = None
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().cup2d_poisson_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def ncells(self) -> int:
+        return int(L.lib().cup2d_poisson_num_cells(self._h))
+
+    def update_mesh(self, mesh: Mesh) -> None:
+        self.mesh = mesh
+        f = mesh.forest()
+        L.check(L.lib().cup2d_poisson_update_mesh(self._h, C.byref(f)), "cup2d_poisson_update_mesh")
+
+    def set_opts(self, opts: Optional[L.SolveOpts] = None, **kw) -> None:
+        self.opts = opts if opts is not None else make_opts(**kw)
+        L.check(L.lib().cup2d_poisson_set_opts(self._h, C.byref(self.opts)), "cup2d_poisson_set_opts")
+
+    def set_grid(self, grid: int) -> None:
+        L.check(L.lib().cup2d_poisson_set_grid(self._h, int(grid)), "cup2d_poisson_set_grid")
+
+    # ------------------------------------------------------------ solve ---
+    def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None) -> np.ndarray:
+        """Host arrays in, host array out (copies inside the call)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        st = L.SolveStats()
+        L.check(L.lib().cup2d_poisson_solve(self._h, _pd(b), _pd(x), C.byref(st)), "cup2d_poisson_solve")
+        self.last_stats = st.as_dict()
+        return x
+
+    def solve_device(self, b, x, stream=None, stats: bool = True) -> Optional[dict]:
+        """Device tensors (torch, float64, contiguous): x holds x0 and receives
+        the solution.  With stats=False the call is asynchronous."""
+        _check_dev(b, self.ncells)
+        _check_dev(x, self.ncells)
+        st = L.SolveStats()
+        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        L.check(L.lib().cup2d_poisson_solve_device(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                                   C.byref(st) if stats else None, s),
+                "cup2d_poisson_solve_device")
+        if stats:
+            self.last_stats = st.as_dict()
+            return self.last_stats
+        return None
+
+    # ------------------------------------------------------ components ---
+    def apply(self, x, y, stream=None) -> None:
+        _check_dev(x, self.ncells)
+        _check_dev(y, self.ncells)
+        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        L.check(L.lib().cup2d_poisson_apply(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s),
+                "cup2d_poisson_apply")
+
+    def precond(self, p, z, stream=None) -> None:
+        fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond
+        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        L.check(fn(self._h, C.c_void_p(p.data_ptr()), C.c_void_p(z.data_ptr()), s), "cup2d_poisson_precond")
+
+    def export_csr(self):
+        n = C.c_int64()
+        nnz = C.c_int64()
+        L.check(L.lib().cup2d_poisson_export_csr(self._h, C.byref(n), C.byref(nnz), None, None, None),
+                "cup2d_poisson_export_csr")
+        rp = np.empty(n.value + 1, dtype=np.int64)
+        col = np.empty(nnz.value, dtype=np.int32)
+        val = np.empty(nnz.value, dtype=np.float64)
+        L.check(L.lib().cup2d_poisson_export_csr(self._h, C.byref(n), C.byref(nnz),
+                                                 rp.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                 col.ctypes.data_as(C.POINTER(C.c_int32)), _pd(val)),
+                "cup2d_poisson_export_csr")
+        return rp, col, val
+
+    def explicit_info(self) -> tuple[int, int]:
+        r = C.c_int64()
+        z = C.c_int64()
+        L.check(L.lib().cup2d_poisson_explicit_info(self._h, C.byref(r), C.byref(z)), "explicit_info")
+        return r.value, z.value
+
+
+def _check_dev(t, n: int) -> None:
+    if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous() and t.numel() == n):
+        raise ValueError(f"expected a contiguous CUDA tensor of {n} elements")
+
+
+def device_pinv() -> np.ndarray:
+    P = np.empty(4096, dtype=np.float64)
+    L.check(L.lib().cup2d_pinv(_pd(P)), "cup2d_pinv")
+    return P.reshape(64, 64)
+
+
+# ------------------------------------------------- reference interface ----
+
+@dataclass
+class ScalarGrid:
+    """A scalar field on a mesh: data[block, iy, ix]."""
+    mesh: Mesh
+    data: object  # numpy (nblocks,8,8) float64, or a CUDA tensor of that shape
+
+    @classmethod
+    def zeros(cls, mesh: Mesh, device=None) -> "ScalarGrid":
+        if device is None:
+            return cls(mesh, np.zeros((mesh.nblocks, 8, 8)))
+        import torch
+        return cls(mesh, torch.zeros((mesh.nblocks, 8, 8), dtype=torch.float64, device=device))
+
+
+@dataclass
+class SimulationData:
+    """The fields of CUP2D's SimulationData that the Poisson path reads
+    (source/Simulation.cpp:239-245, ExpAMRSolver.cpp:366-372)."""
+    mesh: Mesh
+    poissonSolver: str = "cuda_iterative"
+    PoissonTol: float = 1e-6
+    PoissonTolRel: float = 0.0
+    maxPoissonRestarts: int = 30
+    maxPoissonIterations: int = 1000
+    bMeanConstraint: int = 0
+    step: int = 0
+    precision: str = "fp64"
+    UpdateFluxCorrection: bool = True  # set when the mesh changed
+
+
+class PoissonSolver:
+    """Base.h:8-13."""
+
+    def solve(self, input: ScalarGrid, output: ScalarGrid) -> None:  # noqa: A002
+        raise NotImplementedError
+
+
+class ExpAMRSolver(PoissonSolver):
+    """`cuda_iterative`: BiCGSTAB + 64x64 block-Jacobi on the GPU.
+
+    Follows ExpAMRSolver::solve: tolerances are zero and restarts 100 for the
+    first 10 steps (ExpAMRSolver.cpp:366-368), the operator is re-assembled
+    when the mesh changed (UpdateFluxCorrection, :370-376), output holds the
+    initial guess and receives the solution with its volume-weighted mean
+    removed (:383-415)."""
+
+    def __init__(self, sim: SimulationData):
+        if sim.bMeanConstraint:
+            raise NotImplementedError("bMeanConstraint != 0 is not supported by this solver")
+        self.sim = sim
+        self.solver = Solver(sim.mesh, self._opts())
+        sim.UpdateFluxCorrection = False
+
+    def _opts(self) -> L.SolveOpts:
+        s = self.sim
+        early = s.step < 10
+        return make_opts(tol_abs=0.0 if early else s.PoissonTol, tol_rel=0.0 if early else s.PoissonTolRel,
+                         max_restarts=100 if early else s.maxPoissonRestarts, max_iter=s.maxPoissonIterations,
+                         precision=s.precision)
+
+    def solve(self, input: ScalarGrid, output: ScalarGrid) -> None:  # noqa: A002
+        s = self.sim
+        if s.UpdateFluxCorrection:
+            s.UpdateFluxCorrection = False
+            self.solver.update_mesh(s.mesh)
+        self.solver.set_opts(self._opts())
+        if isinstance(input.data, np.ndarray):
+            x = self.solver.solve(input.data.reshape(-1), np.asarray(output.data).reshape(-1))
+            output.data[...] = x.reshape(-1, 8, 8)
+        else:
+            self.solver.solve_device(input.data.reshape(-1), output.data.view(-1))
+
+
+def makePoissonSolver(sim: SimulationData) -> PoissonSolver:
+    """Base.cpp:8-30."""
+    if sim.poissonSolver == "cuda_iterative":
+        return ExpAMRSolver(sim)
+    if sim.poissonSolver == "iterative":
+        raise NotImplementedError('Poisson solver "iterative" (the CPU AMRSolver) is not part of cup2d_b200; '
+                                  'use "cuda_iterative"')
+    raise ValueError(f'Poisson solver: "{sim.poissonSolver}" unrecognized!')

@@ -1,0 +1,169 @@
+/*
+ * cup2d_poisson.h — C ABI of the B200 pressure-Poisson solver.
+ *
+ * Drop-in for CUP2D's GPU Poisson path ("-poissonSolver cuda_iterative"):
+ * BiCGSTAB with the shared 64x64 block-Jacobi preconditioner on the 8x8-cell
+ * block-AMR forest.  Reference interfaces replaced (paths in the CUP2D tree):
+ *
+ *   PoissonSolver::solve(const ScalarGrid*, ScalarGrid*)   source/Poisson/Base.h:12
+ *   makePoissonSolver(SimulationData&)                      source/Poisson/Base.cpp:8-30
+ *   ExpAMRSolver::ExpAMRSolver (P^-1 build)                 source/Poisson/ExpAMRSolver.cpp:25-99
+ *   ExpAMRSolver::getMat (assembly, on flux-correction update)
+ *                                                           source/Poisson/ExpAMRSolver.cpp:180-313,370-376
+ *   ExpAMRSolver::getVec + solve (b, x0, mean removal)      source/Poisson/ExpAMRSolver.cpp:315-416
+ *   LocalSpMatDnVec::solveWithUpdate / solveNoUpdate        source/Poisson/LocalSpMatDnVec.cpp:318-332
+ *   BiCGSTABSolver::main                                    source/Poisson/BiCGSTAB.cu:412-620
+ *
+ * Conventions
+ *   - Cell vectors are FP64, block-major: v[block*64 + iy*8 + ix], blocks in
+ *     the order of the forest passed at creation (CUP2D's blockID order).
+ *   - Every entry point returns a cup2d_status; none exits or aborts.
+ *   - A handle is not thread-safe; it runs its work on one CUDA stream.
+ *   - Pointers named d_* are device pointers on the handle's device; the
+ *     others are host pointers.  `stream` is a cudaStream_t (NULL = the
+ *     handle's own stream).
+ */
+#ifndef CUP2D_POISSON_H
+#define CUP2D_POISSON_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cup2d_status {
+  CUP2D_OK = 0,
+  CUP2D_NOT_CONVERGED = 1,     /* iteration cap reached; best iterate returned */
+  CUP2D_BREAKDOWN_LIMIT = 2,   /* restart cap reached; best iterate returned */
+  CUP2D_BAD_MESH = 3,          /* forest not a valid 2:1-balanced leaf set */
+  CUP2D_OOM = 4,               /* device allocation failed */
+  CUP2D_TIMEOUT = 5,           /* a bounded device-side wait expired */
+  CUP2D_CUDA_ERROR = 6,        /* any other CUDA runtime error */
+  CUP2D_INVALID_ARGUMENT = 7,
+  CUP2D_NO_DEVICE = 8,
+  CUP2D_QUEUE_FULL = 9,        /* serving: no slot / memory for the request now */
+  CUP2D_PENDING = 10           /* serving: request not finished yet */
+} cup2d_status;
+
+typedef enum cup2d_precision {
+  CUP2D_PREC_FP64 = 0,   /* plain FP64 BiCGSTAB: the reference's solve */
+  CUP2D_PREC_MIXED = 1   /* FP32 Krylov vectors and split-TF32 P^-1; FP64 solution
+                            update, true-residual refresh and convergence test */
+} cup2d_precision;
+
+/* The block list Cubism hands to ExpAMRSolver::getMat. */
+typedef struct cup2d_forest {
+  int32_t bpdx, bpdy;            /* root blocks per direction (-bpdx, -bpdy) */
+  int32_t level_max;             /* number of levels (-levelMax) */
+  int32_t periodic_x, periodic_y;/* 1 periodic, 0 wall (homogeneous Neumann) */
+  double extent;                 /* longer domain side (-extent) */
+  int64_t nblocks;
+  const int32_t* level;          /* [nblocks] refinement level of each block */
+  const int32_t* bx;             /* [nblocks] block index at its level, x */
+  const int32_t* by;             /* [nblocks] block index at its level, y */
+} cup2d_forest;
+
+/* Solver options: SimulationData's Poisson fields plus the additions. */
+typedef struct cup2d_solve_opts {
+  double tol_abs;          /* sim.PoissonTol (max_error) */
+  double tol_rel;          /* sim.PoissonTolRel (max_rel_error) */
+  int32_t max_restarts;    /* sim.maxPoissonRestarts */
+  int32_t max_iter;        /* BiCGSTAB.cu:468 fixes 1000 */
+  int32_t precision;       /* cup2d_precision */
+  int32_t subtract_mean;   /* 1: x -= sum(h^2 x)/sum(h^2) after the solve */
+  double reliable_delta;   /* mixed: once the FP32 residual has dropped by this factor
+                              since the last replacement, replace it by the true FP64
+                              residual b - A x */
+  int32_t timeout_ms;      /* bound on every device-side wait */
+  int32_t reliable_restart;/* mixed: 1 restarts the BiCGSTAB recurrences (rhat = r,
+                              p = nu = 0) at each replacement: FP64 iterative
+                              refinement of restarted FP32 BiCGSTAB sweeps whose
+                              solution update is accumulated in FP64; 0 keeps the
+                              recurrences running (reliable updates) */
+} cup2d_solve_opts;
+
+typedef struct cup2d_solve_stats {
+  int32_t status;          /* cup2d_status of this solve */
+  int32_t iterations;      /* BiCGSTAB iterations (summed over inner solves) */
+  int32_t restarts;
+  int32_t refinements;     /* mixed: FP64 true-residual replacements taken */
+  double err_init;         /* |b - A x0|_inf */
+  double err_final;        /* fp64: best recursive |r|_inf (the reference's test);
+                              mixed: final true |b - A x|_inf in FP64 */
+  double rel_res_inf;      /* err_final / err_init */
+  double solve_ms;         /* device time of the solve (CUDA events) */
+} cup2d_solve_stats;
+
+typedef struct cup2d_poisson cup2d_poisson;
+
+/* ------------------------------------------------------------ library ---- */
+const char* cup2d_version(void);
+const char* cup2d_status_string(int status);
+void cup2d_default_opts(cup2d_solve_opts* opts);
+/* Copies the 64x64 row-major P^-1 = -K^-1 built on the device (FP64). */
+int cup2d_pinv(double* P_out);
+
+/* ------------------------------------------------------------ solver ----- */
+/* makePoissonSolver + ExpAMRSolver ctor + first getMat: builds P^-1 and the
+ * operator on the device. */
+int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opts,
+                         cup2d_poisson** out);
+/* Re-assembly after mesh adaptation (the UpdateFluxCorrection branch). */
+int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest);
+int cup2d_poisson_set_opts(cup2d_poisson* h, const cup2d_solve_opts* opts);
+int64_t cup2d_poisson_num_cells(const cup2d_poisson* h);
+/* Number of CTAs of the persistent solve kernels (0 = size heuristic).  The
+ * launch is clamped to what fits co-resident on the device. */
+int cup2d_poisson_set_grid(cup2d_poisson* h, int32_t grid);
+int cup2d_poisson_destroy(cup2d_poisson* h);
+
+/* PoissonSolver::solve: b is the RHS (sim.tmp), x holds x0 on entry and the
+ * solution on exit (sim.pres).  Host buffers: copies are part of the call. */
+int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x,
+                        cup2d_solve_stats* stats);
+/* Same on device buffers, asynchronous on `stream` unless stats != NULL
+ * (stats are read back after the solve, which synchronises the stream). */
+int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
+                               cup2d_solve_stats* stats, void* stream);
+
+/* Building blocks (device buffers), exposed for parity tests. */
+int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream);
+int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
+/* FP32 P^-1 apply of the mixed form (split-TF32 tensor-core MMA). */
+int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);
+/* The assembled operator as CSR (host buffers).  Call with NULL arrays to
+ * get n and nnz. */
+int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n, int64_t* nnz,
+                             int64_t* row_ptr, int32_t* col, double* val);
+/* Explicit (coarse/fine) rows only: number of rows and non-zeros. */
+int cup2d_poisson_explicit_info(cup2d_poisson* h, int64_t* rows, int64_t* nnz);
+
+/* ------------------------------------------------- synthetic problems ---- */
+typedef struct cup2d_mesh cup2d_mesh;
+/* Forest refined to the finest level where a block meets the band
+ * | |p - c| - r | <= band of any disk (cx, cy, r triples), 2:1 balanced,
+ * Morton ordered.  The mesh owns the arrays that cup2d_mesh_forest exposes. */
+int cup2d_mesh_disks(int32_t bpdx, int32_t bpdy, int32_t level_max, double extent,
+                     int32_t periodic_x, int32_t periodic_y, int32_t ndisks,
+                     const double* disks, double band, cup2d_mesh** out);
+int cup2d_mesh_uniform(int32_t bpdx, int32_t bpdy, int32_t level_max, int32_t level,
+                       double extent, int32_t periodic_x, int32_t periodic_y,
+                       cup2d_mesh** out);
+int cup2d_mesh_forest(const cup2d_mesh* m, cup2d_forest* out);
+int cup2d_mesh_destroy(cup2d_mesh* m);
+/* 0 if the forest is a valid 2:1-balanced leaf set, else CUP2D_BAD_MESH. */
+int cup2d_forest_validate(const cup2d_forest* f);
+/* Cell size of each block: h = extent / (max(bpdx,bpdy) * 8 * 2^level). */
+int cup2d_forest_cell_h(const cup2d_forest* f, double* h_out);
+/* Seeded Fourier-velocity divergence RHS, zero entry-sum (n = 64*nblocks). */
+int cup2d_rhs_fourier(const cup2d_forest* f, uint64_t seed, int32_t kmax, double* b);
+int32_t cup2d_fourier_num_modes(int32_t kmax);
+int cup2d_fourier_coefs(uint64_t seed, int32_t kmax, double* coef);
+int cup2d_fourier_advance(uint64_t seed, int32_t kmax, double rho, int64_t step, double* coef);
+int cup2d_rhs_from_coefs(const cup2d_forest* f, int32_t kmax, const double* coef, double* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUP2D_POISSON_H */
