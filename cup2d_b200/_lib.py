@@ -62,6 +62,8 @@ SIGNATURES = {
     "cup2d_poisson_precond32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_export_csr": (C.c_int, [C.c_void_p, P_i64, P_i64, P_i64, P_i32, P_f64]),
     "cup2d_poisson_explicit_info": (C.c_int, [C.c_void_p, P_i64, P_i64]),
+    "cup2d_poisson_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cup2d_poisson_profile": (C.c_int, [C.c_void_p, P_f64, P_f64, C.c_int32]),
     "cup2d_mesh_disks": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                    C.c_int32, P_f64, C.c_double, C.POINTER(C.c_void_p)]),
     "cup2d_mesh_uniform": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,

@@ -217,6 +217,13 @@ __global__ void k_classify(ForestDev F, int32_t* __restrict__ nbr, unsigned long
   hblk[b] = h0 / (double)(1ll << l);
 }
 
+// SpMV cost of each block: the stencil rows plus one per explicit row; its
+// prefix sum partitions the SpMV passes across CTAs.
+__global__ void k_spmv_cost(const int32_t* __restrict__ xcount, int64_t nb, int32_t* __restrict__ w) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (b < nb) w[b] = kSpmvBlockCost + xcount[b];
+}
+
 // ------------------------------------------------------------- scans ------
 
 // Exclusive scan of int32 counts into int32 offsets (out[n] = total), in
@@ -477,8 +484,9 @@ __device__ void build_row(const ForestDev& Fd, int64_t b, int ix, int iy, RowAcc
 // length, pass 1 the row.
 __global__ void __launch_bounds__(64) k_rows(ForestDev Fd, const unsigned long long* __restrict__ xmask,
                                              const int32_t* __restrict__ xbase, int32_t* __restrict__ rowlen,
-                                             const int32_t* __restrict__ xptr, int32_t* __restrict__ xcol,
-                                             double* __restrict__ xval, int pass, int* __restrict__ err) {
+                                             int32_t* __restrict__ rowcell, const int32_t* __restrict__ xptr,
+                                             int32_t* __restrict__ xcol, double* __restrict__ xval, int pass,
+                                             int* __restrict__ err) {
   const int64_t b = blockIdx.x;
   const int c = threadIdx.x;
   const unsigned long long m = xmask[b];
@@ -488,6 +496,7 @@ __global__ void __launch_bounds__(64) k_rows(ForestDev Fd, const unsigned long l
   build_row(Fd, b, c & 7, c >> 3, row, err);
   if (pass == 0) {
     rowlen[r] = row.n;
+    rowcell[r] = (int32_t)(b * kBLEN + c);
   } else {
     const int32_t o = xptr[r];
     for (int k = 0; k < row.n; ++k) {
@@ -526,6 +535,8 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   k_fill_tables<<<g, 256, 0, s>>>(F, out.table, out.err);
   k_classify<<<g, 256, 0, s>>>(F, out.nbr, out.xmask, out.xcount, out.hblk, in.h0, out.err);
   launch_exclusive_scan(out.xcount, nb, out.xbase, out.scan_tmp, s);
+  k_spmv_cost<<<g, 256, 0, s>>>(out.xcount, nb, out.wcost);
+  launch_exclusive_scan(out.wcost, nb, out.wprefix, out.scan_tmp, s);
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
   int32_t hR = 0;
   int herr = 0;
@@ -538,7 +549,8 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   int st = out.alloc_rows(out.ctx, hR);
   if (st != CUP2D_OK) return st;
   if (hR > 0) {
-    k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, nullptr, nullptr, nullptr, 0, out.err);
+    k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.rowcell, nullptr, nullptr, nullptr,
+                                       0, out.err);
     launch_exclusive_scan(out.rowlen, hR, out.xptr, out.scan_tmp, s);
   } else {
     cudaMemsetAsync(out.xptr, 0, sizeof(int32_t), s);
@@ -554,7 +566,8 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   st = out.alloc_nnz(out.ctx, hnnz);
   if (st != CUP2D_OK) return st;
   if (hR > 0) {
-    k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.xptr, out.xcol, out.xval, 1, out.err);
+    k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.rowcell, out.xptr, out.xcol,
+                                       out.xval, 1, out.err);
     launch_convert_f64_f32(out.xval, out.xval32, hnnz, s);
   }
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;

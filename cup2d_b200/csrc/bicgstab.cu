@@ -48,6 +48,7 @@ namespace {
 
 constexpr int kWarps = kSolveThreads / 32;
 constexpr int kPad = 68;  // staged block row (conflict-free fragment loads)
+constexpr int kMaxSweep = 64;  // mixed: longest FP32 sweep between true residuals
 
 enum : int {
   Q_INIT = 0,   // 3: |A x0|_inf, |r0|_inf, |r0|^2
@@ -60,7 +61,14 @@ enum : int {
 };
 static_assert(Q_SUMB + 1 <= kRedQ, "reduction slots");
 
+// P^-1 operand in shared memory: FP64 rows, or the TF32 split (hi, lo)
+union PinvSmem {
+  double d[kBLEN][kPad];
+  uint32_t f[2][kBLEN][kPad];
+};
+
 struct Smem {
+  PinvSmem P;
   union {
     double d[2][8][kPad];
     float f[2][16][kPad];
@@ -126,26 +134,29 @@ __device__ __forceinline__ void grid_reduce(Smem& sm, unsigned is_max, const dou
 template <class T>
 struct Pinv;
 
-// FP64: tiles of 8 blocks; warp w computes rows 8w..8w+7 with DMMA m8n8k4,
-// P^-1 fragments (16 per lane) in registers for the whole solve.
+// FP64: tiles of 8 blocks; warp w computes rows 8w..8w+7 with DMMA m8n8k4.
+// P^-1 stays in shared memory with padded rows: the A-fragment loads
+// (lane g,t reads row 8w+g, column 4kk+t) hit every bank pair once per
+// 16 lanes, the minimum two wavefronts for 32 doubles.
 template <>
 struct Pinv<double> {
   static constexpr int kTile = 8;
-  double af[16];
-  __device__ __forceinline__ void load(const double* __restrict__ P, const float*, int w, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) af[kk] = __ldg(P + (8 * w + g) * kBLEN + 4 * kk + t);
+  const double (*P)[kPad];
+  // all threads; the caller synchronises before the first apply
+  __device__ __forceinline__ void load(PinvSmem& s, const double* __restrict__ Pg, const float*) {
+    for (int q = threadIdx.x; q < kBLEN * kBLEN; q += blockDim.x) s.d[q / kBLEN][q % kBLEN] = __ldg(Pg + q);
+    P = s.d;
   }
   __device__ __forceinline__ static double (*rows(Smem& sm, int buf))[kPad] { return sm.tile.d[buf]; }
   __device__ __forceinline__ void apply(const double (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
                                         double* __restrict__ z) const {
     const int g = lane >> 2, t = lane & 3;
+    const double* arow = P[8 * w + g];
     double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
 #pragma unroll
     for (int kk = 0; kk < 16; kk += 2) {
-      dmma_884(c0, c1, af[kk], tile[g][4 * kk + t]);
-      dmma_884(e0, e1, af[kk + 1], tile[g][4 * (kk + 1) + t]);
+      dmma_884(c0, c1, arow[4 * kk + t], tile[g][4 * kk + t]);
+      dmma_884(e0, e1, arow[4 * (kk + 1) + t], tile[g][4 * (kk + 1) + t]);
     }
     c0 += e0;
     c1 += e1;
@@ -175,21 +186,19 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 template <>
 struct Pinv<float> {
   static constexpr int kTile = 16;
-  uint32_t ahi[8][4], alo[8][4];
-  __device__ __forceinline__ void load(const double*, const float* __restrict__ P32, int w, int lane) {
-    const int g = lane >> 2, t = lane & 3, m = w & 3;
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-      const float v[4] = {__ldg(P32 + (16 * m + g) * kBLEN + 8 * kk + t),
-                          __ldg(P32 + (16 * m + g + 8) * kBLEN + 8 * kk + t),
-                          __ldg(P32 + (16 * m + g) * kBLEN + 8 * kk + t + 4),
-                          __ldg(P32 + (16 * m + g + 8) * kBLEN + 8 * kk + t + 4)};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        ahi[kk][q] = to_tf32(v[q]);
-        alo[kk][q] = to_tf32(v[q] - __uint_as_float(ahi[kk][q]));
-      }
+  const uint32_t (*Ph)[kPad];
+  const uint32_t (*Pl)[kPad];
+  // all threads; the caller synchronises before the first apply.  The split
+  // P = Phi + Plo (TF32 bit patterns) is formed once.
+  __device__ __forceinline__ void load(PinvSmem& s, const double*, const float* __restrict__ P32) {
+    for (int q = threadIdx.x; q < kBLEN * kBLEN; q += blockDim.x) {
+      const float v = __ldg(P32 + q);
+      const uint32_t hi = to_tf32(v);
+      s.f[0][q / kBLEN][q % kBLEN] = hi;
+      s.f[1][q / kBLEN][q % kBLEN] = to_tf32(v - __uint_as_float(hi));
     }
+    Ph = s.f[0];
+    Pl = s.f[1];
   }
   __device__ __forceinline__ static float (*rows(Smem& sm, int buf))[kPad] { return sm.tile.f[buf]; }
   __device__ __forceinline__ void apply(const float (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
@@ -197,14 +206,20 @@ struct Pinv<float> {
     const int g = lane >> 2, t = lane & 3, m = w & 3, nt = w >> 2;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     const float* brow = tile[8 * nt + g];
+    const int ra = 16 * m + g, rb = ra + 8;
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
-      const float x0 = brow[8 * kk + t], x1 = brow[8 * kk + t + 4];
+      const int c = 8 * kk + t;
+      // A fragment rows ra/rb, columns c/c+4: word address 4*row + col mod 32
+      // differs across the 32 lanes (row stride 68 words), conflict-free
+      const uint32_t ahi[4] = {Ph[ra][c], Ph[rb][c], Ph[ra][c + 4], Ph[rb][c + 4]};
+      const uint32_t alo[4] = {Pl[ra][c], Pl[rb][c], Pl[ra][c + 4], Pl[rb][c + 4]};
+      const float x0 = brow[c], x1 = brow[c + 4];
       const uint32_t h0 = to_tf32(x0), h1 = to_tf32(x1);
       const uint32_t l0 = to_tf32(x0 - __uint_as_float(h0)), l1 = to_tf32(x1 - __uint_as_float(h1));
-      mma_tf32(acc, alo[kk], h0, h1);
-      mma_tf32(acc, ahi[kk], l0, l1);
-      mma_tf32(acc, ahi[kk], h0, h1);
+      mma_tf32(acc, alo, h0, h1);
+      mma_tf32(acc, ahi, l0, l1);
+      mma_tf32(acc, ahi, h0, h1);
     }
     const int n0 = 8 * nt + 2 * t, n1 = n0 + 1;
     const int r0 = 16 * m + g, r1 = r0 + 8;
@@ -253,18 +268,16 @@ __device__ __forceinline__ double dprod(float a, float b) { return (double)a * (
 __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
                                               double mean_b, const double* __restrict__ x, float* __restrict__ r,
                                               float* __restrict__ rh, bool set_rh, double* __restrict__ red,
-                                              int64_t b0, int64_t b1) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-    const int64_t o = blk * kBLEN;
-    const double x0 = __ldcg(x + o + lane), x1 = __ldcg(x + o + lane + 32);
-    double y[2];
-    spmv_block<double>(M, blk, x, lane, x0, x1, y[0], y[1]);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int64_t i = o + lane + 32 * h;
-      const double r64 = (__ldg(b + i) - mean_b) - y[h];
+                                              int64_t sb0, int64_t sb1) {
+  struct Epi {
+    const double* b;
+    double mean_b;
+    float* r;
+    float* rh;
+    bool set_rh;
+    double v[5];
+    __device__ __forceinline__ void operator()(int64_t i, double y) {
+      const double r64 = (__ldg(b + i) - mean_b) - y;
       const float r32 = (float)r64;
       r[i] = r32;
       float rhv;
@@ -280,8 +293,9 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       v[3] += dprod(rhv, rhv);
       v[4] = nanmax(v[4], fabs((double)r32));
     }
-  }
-  cta_partials<5>(sm, v, 0x11u, red, Q_RU);
+  } epi{b, mean_b, r, rh, set_rh, {0.0, 0.0, 0.0, 0.0, 0.0}};
+  spmv_range<double>(M, x, sb0, sb1, epi);
+  cta_partials<5>(sm, epi.v, 0x11u, red, Q_RU);
 }
 
 struct MixedCtx {  // what the reliable update needs
@@ -299,8 +313,8 @@ struct MixedCtx {  // what the reliable update needs
 template <class T, class X, bool RU>
 __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const Pinv<T>& pin,
                               const Vecs<T, X> V, double* __restrict__ red, int64_t b0, int64_t b1,
-                              double tol_abs, double tol_rel, int max_restarts, int max_iter, const MixedCtx& mx,
-                              IterState& st) {
+                              int64_t sb0, int64_t sb1, double tol_abs, double tol_rel, int max_restarts,
+                              int max_iter, const MixedCtx& mx, IterState& st) {
   constexpr int TB = Pinv<T>::kTile;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const double eps = 1e-21;
@@ -308,6 +322,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
   bool zero_pnu = true;
   double rho = st.rho, nr = st.nr, nrh = st.nrh;
   double rmax_since = sqrt(nr);  // largest |r|_2 since the last true residual
+  int since = 0;                 // iterations since the last true residual
   int k;
   st.status = CUP2D_NOT_CONVERGED;
   for (k = 0; k < max_iter; ++k) {
@@ -357,22 +372,23 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       }
       zero_pnu = false;
     }
-    if (!B.sync(&sm.flag)) return false;
+    if (!B.sync(&sm.flag, 1)) return false;
     // pass B: nu = A z; (rhat, nu)
     {
-      double v[1] = {0.0};
-      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-        const int64_t o = blk * kBLEN;
-        const T z0 = __ldcg(V.z + o + lane), z1 = __ldcg(V.z + o + lane + 32);
-        T y0, y1;
-        spmv_block<T>(M, blk, V.z, lane, z0, z1, y0, y1);
-        V.nu[o + lane] = y0;
-        V.nu[o + lane + 32] = y1;
-        v[0] += dprod(__ldcg(V.rh + o + lane), y0) + dprod(__ldcg(V.rh + o + lane + 32), y1);
-      }
+      struct Epi {
+        const T* rh;
+        T* nu;
+        double acc;
+        __device__ __forceinline__ void operator()(int64_t i, T y) {
+          nu[i] = y;
+          acc += dprod(__ldcg(rh + i), y);
+        }
+      } epi{V.rh, V.nu, 0.0};
+      spmv_range<T>(M, V.z, sb0, sb1, epi);
+      const double v[1] = {epi.acc};
       cta_partials<1>(sm, v, 0u, red, Q_RHNU);
     }
-    if (!B.sync(&sm.flag)) return false;
+    if (!B.sync(&sm.flag, 2)) return false;
     grid_reduce<1>(sm, 0u, red, Q_RHNU);
     alpha = rho / (sm.gres[0] + eps);
     const T ta = (T)alpha;
@@ -405,23 +421,24 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
         buf ^= 1;
       }
     }
-    if (!B.sync(&sm.flag)) return false;
+    if (!B.sync(&sm.flag, 3)) return false;
     // pass D: t = A z; (t,s), (t,t)
     {
-      double v[2] = {0.0, 0.0};
-      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-        const int64_t o = blk * kBLEN;
-        const T z0 = __ldcg(V.z + o + lane), z1 = __ldcg(V.z + o + lane + 32);
-        T y0, y1;
-        spmv_block<T>(M, blk, V.z, lane, z0, z1, y0, y1);
-        V.t[o + lane] = y0;
-        V.t[o + lane + 32] = y1;
-        v[0] += dprod(y0, __ldcg(V.r + o + lane)) + dprod(y1, __ldcg(V.r + o + lane + 32));
-        v[1] += dprod(y0, y0) + dprod(y1, y1);
-      }
+      struct Epi {
+        const T* s;
+        T* t;
+        double ts, tt;
+        __device__ __forceinline__ void operator()(int64_t i, T y) {
+          t[i] = y;
+          ts += dprod(y, __ldcg(s + i));
+          tt += dprod(y, y);
+        }
+      } epi{V.r, V.t, 0.0, 0.0};
+      spmv_range<T>(M, V.z, sb0, sb1, epi);
+      const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
     }
-    if (!B.sync(&sm.flag)) return false;
+    if (!B.sync(&sm.flag, 4)) return false;
     grid_reduce<2>(sm, 0u, red, Q_TS);
     omega = sm.gres[0] / (sm.gres[1] + eps);
     const T to = (T)omega;
@@ -445,7 +462,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       }
       cta_partials<4>(sm, v, 0x1u, red, Q_RMAX);
     }
-    if (!B.sync(&sm.flag)) return false;
+    if (!B.sync(&sm.flag, 5)) return false;
     grid_reduce<4>(sm, 0x1u, red, Q_RMAX);
     double error = sm.gres[0];
     double rho_new = sm.gres[1];
@@ -459,11 +476,15 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     bool refreshed = false;
     if constexpr (RU) {
       rmax_since = fmax(rmax_since, sqrt(nr));
+      ++since;
       const bool claims = (error <= tol_abs) || (error / st.err_init <= tol_rel);
-      if (claims || sqrt(nr) < mx.delta * rmax_since) {
+      // refresh when the FP32 residual dropped by delta, claims convergence,
+      // or a sweep stalls for kMaxSweep iterations
+      if (claims || sqrt(nr) < mx.delta * rmax_since || since >= kMaxSweep) {
+        since = 0;
         // pass E's barrier already ordered every CTA's x update before this
-        true_residual(sm, M, mx.b, mx.mean_b, V.x, V.r, V.rh, mx.restart, red, b0, b1);
-        if (!B.sync(&sm.flag)) return false;
+        true_residual(sm, M, mx.b, mx.mean_b, V.x, V.r, V.rh, mx.restart, red, sb0, sb1);
+        if (!B.sync(&sm.flag, 6)) return false;
         grid_reduce<5>(sm, 0x11u, red, Q_RU);
         ++st.updates;
         refreshed = true;
@@ -521,7 +542,7 @@ __device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, doubl
     v[1] += 2.0 * (hb * hb);
   }
   cta_partials<2>(sm, v, 0u, red, Q_HX);
-  if (!B.sync(&sm.flag)) return false;
+  if (!B.sync(&sm.flag, 7)) return false;
   grid_reduce<2>(sm, 0u, red, Q_HX);
   const double avg = sm.gres[0] / sm.gres[1];
   for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
@@ -548,35 +569,41 @@ __device__ __forceinline__ void take_best(bool best_is_x, double* __restrict__ x
 
 // ====================================================== plain FP64 ========
 
-__global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab64(SolveArgs64 S) {
+// Three CTAs per SM (80 registers): the passes are bound by per-warp memory
+// latency, and the extra warps outweigh the spills this costs (measured on
+// the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(SolveArgs64 S) {
   __shared__ Smem sm;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t nb = S.M.nb;
   const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u};
+  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   Pinv<double> pin;
-  pin.load(S.P, nullptr, w, lane);
+  pin.load(sm.P, S.P, nullptr);
+  __syncthreads();
   const MeshView& M = S.M;
   const Vecs<double, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
 
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
   {
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-      const int64_t o = blk * kBLEN;
-      const double x0 = __ldcg(S.x + o + lane), x1 = __ldcg(S.x + o + lane + 32);
-      double y0, y1;
-      spmv_block<double>(M, blk, S.x, lane, x0, x1, y0, y1);
-      const double r0 = __ldg(S.b + o + lane) - y0, r1 = __ldg(S.b + o + lane + 32) - y1;
-      S.r[o + lane] = r0; S.r[o + lane + 32] = r1;
-      S.rh[o + lane] = r0; S.rh[o + lane + 32] = r1;
-      v[0] = nanmax(v[0], nanmax(fabs(y0), fabs(y1)));
-      v[1] = nanmax(v[1], nanmax(fabs(r0), fabs(r1)));
-      v[2] += r0 * r0 + r1 * r1;
-    }
-    cta_partials<3>(sm, v, 0x3u, S.red, Q_INIT);
+    struct Epi {
+      const double* b;
+      double* r;
+      double* rh;
+      double v[3];
+      __device__ __forceinline__ void operator()(int64_t i, double y) {
+        const double rv = __ldg(b + i) - y;
+        r[i] = rv;
+        rh[i] = rv;
+        v[0] = nanmax(v[0], fabs(y));
+        v[1] = nanmax(v[1], fabs(rv));
+        v[2] += rv * rv;
+      }
+    } epi{S.b, S.r, S.rh, {0.0, 0.0, 0.0}};
+    spmv_range<double>(M, S.x, sb0, sb1, epi);
+    cta_partials<3>(sm, epi.v, 0x3u, S.red, Q_INIT);
   }
-  if (!B.sync(&sm.flag)) return;
+  if (!B.sync(&sm.flag, 0)) return;
   grid_reduce<3>(sm, 0x3u, S.red, Q_INIT);
   IterState st;
   const double norm_ax0 = sm.gres[0];
@@ -590,7 +617,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab64(SolveArgs64 S) 
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
   const MixedCtx none{};
-  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, S.red, b0, b1, S.tol_abs, S.tol_rel,
+  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, S.red, b0, b1, sb0, sb1, S.tol_abs, S.tol_rel,
                                             S.max_restarts, S.max_iter, none, st))
     return;
   take_best(st.best_is_x, S.x, S.xo, b0, b1);
@@ -608,14 +635,16 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab64(SolveArgs64 S) 
 
 // ================================================ mixed precision =========
 
-__global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab_mixed(SolveArgsMixed S) {
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
   __shared__ Smem sm;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t nb = S.M.nb;
   const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u};
+  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   Pinv<float> pin;
-  pin.load(nullptr, S.P32, w, lane);
+  pin.load(sm.P, nullptr, S.P32);
+  __syncthreads();
   const Vecs<float, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
 
   // Neumann compatibility: project b to zero sum (sum b / n)
@@ -627,7 +656,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab_mixed(SolveArgsMi
     }
     cta_partials<1>(sm, v, 0u, S.red, Q_SUMB);
   }
-  if (!B.sync(&sm.flag)) return;
+  if (!B.sync(&sm.flag, 8)) return;
   grid_reduce<1>(sm, 0u, S.red, Q_SUMB);
   MixedCtx mx;
   mx.b = S.b;
@@ -636,8 +665,8 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab_mixed(SolveArgsMi
   mx.tol_abs = S.tol_abs;
   mx.tol_rel = S.tol_rel;
   mx.restart = S.reliable_restart != 0;
-  true_residual(sm, S.M, S.b, mx.mean_b, S.x, S.r, S.rh, true, S.red, b0, b1);
-  if (!B.sync(&sm.flag)) return;
+  true_residual(sm, S.M, S.b, mx.mean_b, S.x, S.r, S.rh, true, S.red, sb0, sb1);
+  if (!B.sync(&sm.flag, 0)) return;
   grid_reduce<5>(sm, 0x11u, S.red, Q_RU);
   IterState st;
   st.err_init = sm.gres[0];
@@ -654,7 +683,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_bicgstab_mixed(SolveArgsMi
   const bool done0 = st.err_true <= S.tol_abs || st.err_true == 0.0;
   if (done0) {
     st.status = CUP2D_OK;
-  } else if (!bicgstab_loop<float, double, true>(sm, B, S.M, pin, V, S.red, b0, b1, S.tol_abs, S.tol_rel,
+  } else if (!bicgstab_loop<float, double, true>(sm, B, S.M, pin, V, S.red, b0, b1, sb0, sb1, S.tol_abs, S.tol_rel,
                                                  S.max_restarts, S.max_iter, mx, st)) {
     return;
   }
@@ -702,9 +731,8 @@ __global__ void __launch_bounds__(256) k_spmv64(MeshView M, const double* __rest
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t blk = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); blk < M.nb; blk += warps) {
     const int64_t o = blk * kBLEN;
-    const double x0 = x[o + lane], x1 = x[o + lane + 32];
     double y0, y1;
-    spmv_block<double>(M, blk, x, lane, x0, x1, y0, y1);
+    spmv_block<double>(M, blk, x, lane, y0, y1);
     y[o + lane] = y0;
     y[o + lane + 32] = y1;
   }
@@ -720,9 +748,11 @@ cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStr
 __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int64_t nb,
                                                              const double* __restrict__ p, double* __restrict__ z) {
   __shared__ double tile[8][kPad];
+  __shared__ PinvSmem Ps;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Pinv<double> pin;
-  pin.load(P, nullptr, w, lane);
+  pin.load(Ps, P, nullptr);
+  __syncthreads();
   for (int64_t tb = (int64_t)blockIdx.x * 8; tb < nb; tb += (int64_t)gridDim.x * 8) {
     const int nvalid = (int)imin64(8, nb - tb);
     if (w < nvalid) {
@@ -748,9 +778,11 @@ cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, doubl
 __global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __restrict__ P32, int64_t nb,
                                                              const float* __restrict__ p, float* __restrict__ z) {
   __shared__ float tile[16][kPad];
+  __shared__ PinvSmem Ps;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Pinv<float> pin;
-  pin.load(nullptr, P32, w, lane);
+  pin.load(Ps, nullptr, P32);
+  __syncthreads();
   for (int64_t tb = (int64_t)blockIdx.x * 16; tb < nb; tb += (int64_t)gridDim.x * 16) {
     const int nvalid = (int)imin64(16, nb - tb);
     for (int j = w; j < 16; j += kWarps) {

@@ -78,7 +78,7 @@ struct cup2d_poisson {
   double extent = 1.0;
   int64_t nb = 0;
   // operator
-  DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol;
+  DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol, wcost, wprefix, rowcell;
   DevBuf<unsigned long long> xmask;
   DevBuf<double> hblk, xval, P;
   DevBuf<float> xval32, P32;
@@ -93,6 +93,15 @@ struct cup2d_poisson {
   DevBuf<unsigned> bar;
   DevBuf<int> abort_flag;
   DevBuf<DevStats> dstats;
+  DevBuf<unsigned long long> prof;  // phase timers (profiling on)
+  // SpMV partition: cost prefix of the current mesh and ranges per grid
+  std::vector<int32_t> wprefix_host;
+  std::vector<int32_t> sbounds_host;
+  DevBuf<int32_t> sbounds;
+  int sb_grid = 0;
+  uint64_t mesh_version = 0, sb_version = ~0ull;
+  bool profiling = false;
+  int prof_grid = 0;                // grid of the profiled solves
   DevStats* hstats = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int grid64 = 0, gridmx = 0;      // max co-resident grids
@@ -114,8 +123,11 @@ int alloc_rows_cb(void* ctx, int64_t R) {
   if (st) return st;
   st = h->xptr.ensure(R + 1);
   if (st) return st;
+  st = h->rowcell.ensure(R);
+  if (st) return st;
   h->mesh.rowlen = h->rowlen.p;
   h->mesh.xptr = h->xptr.p;
+  h->mesh.rowcell = h->rowcell.p;
   return CUP2D_OK;
 }
 
@@ -151,7 +163,8 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb)) ||
       (st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
       (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
-      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
+      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)) ||
+      (st = h->wcost.ensure(nb)) || (st = h->wprefix.ensure(nb + 1)))
     return st;
   // Krylov vectors
   if ((st = h->xo.ensure(n)) || (st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) ||
@@ -173,6 +186,8 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   m.xcount = h->xcount.p;
   m.xbase = h->xbase.p;
   m.hblk = h->hblk.p;
+  m.wcost = h->wcost.p;
+  m.wprefix = h->wprefix.p;
   m.scan_tmp = h->scan_tmp.p;
   m.err = h->err.p;
   m.ctx = h;
@@ -184,6 +199,12 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
                 f->extent / ((double)std::max(f->bpdx, f->bpdy) * 8.0)};
   st = assemble_on_device(in, m, s);
   if (st) return st;
+  h->wprefix_host.resize(nb + 1);
+  if (cudaMemcpyAsync(h->wprefix_host.data(), h->wprefix.p, sizeof(int32_t) * (nb + 1), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  ++h->mesh_version;
   h->bpdx = f->bpdx;
   h->bpdy = f->bpdy;
   h->level_max = f->level_max;
@@ -200,6 +221,29 @@ int ensure_scratch(cup2d_poisson* h) {
   if ((st = h->red.ensure((int64_t)kRedQ * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
       (st = h->abort_flag.ensure(1)) || (st = h->dstats.ensure(1)))
     return st;
+  return CUP2D_OK;
+}
+
+// Block ranges of the SpMV passes for `grid` CTAs: CTA c takes the blocks
+// whose cost prefix falls in [W*c/grid, W*(c+1)/grid).
+int ensure_sbounds(cup2d_poisson* h, int grid, cudaStream_t s) {
+  if (h->sb_grid == grid && h->sb_version == h->mesh_version) return CUP2D_OK;
+  int st = h->sbounds.ensure(grid + 1);
+  if (st) return st;
+  const std::vector<int32_t>& wp = h->wprefix_host;
+  const int64_t W = wp.back();
+  h->sbounds_host.resize(grid + 1);
+  for (int c = 0; c <= grid; ++c) {
+    const int64_t target = W * c / grid;
+    h->sbounds_host[c] = (int32_t)(std::lower_bound(wp.begin(), wp.end(), (int32_t)target) - wp.begin());
+  }
+  h->sbounds_host[grid] = (int32_t)h->nb;
+  if (cudaMemcpyAsync(h->sbounds.p, h->sbounds_host.data(), sizeof(int32_t) * (grid + 1), cudaMemcpyHostToDevice,
+                      s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  h->sb_grid = grid;
+  h->sb_version = h->mesh_version;
   return CUP2D_OK;
 }
 
@@ -255,7 +299,7 @@ void cup2d_default_opts(cup2d_solve_opts* o) {
   o->max_iter = 1000;
   o->precision = CUP2D_PREC_FP64;
   o->subtract_mean = 1;
-  o->reliable_delta = 0.1;
+  o->reliable_delta = 0.5;
   o->reliable_restart = 1;
   o->timeout_ms = 20000;
 }
@@ -344,7 +388,8 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   if (!h) return CUP2D_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   DevBuf<int32_t>* i32[] = {&h->level, &h->bx, &h->by, &h->table, &h->nbr, &h->xcount, &h->xbase,
-                            &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol};
+                            &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol, &h->wcost, &h->wprefix,
+                            &h->rowcell};
   for (auto* b : i32) b->release();
   h->xmask.release();
   DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
@@ -357,6 +402,8 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   h->bar.release();
   h->abort_flag.release();
   h->dstats.release();
+  h->prof.release();
+  h->sbounds.release();
   if (h->hstats) cudaFreeHost(h->hstats);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -368,7 +415,7 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
 int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x, cup2d_solve_stats* stats,
                                void* stream) {
   if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   const cup2d_solve_opts& o = h->opts;
   int st;
   if ((st = ensure_scratch(h))) return st;
@@ -380,6 +427,18 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
   const int grid = o.precision == CUP2D_PREC_MIXED ? h->grid_for(h->gridmx) : h->grid_for(h->grid64);
   const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
+  if ((st = ensure_sbounds(h, grid, s))) return st;
+  unsigned long long* prof = nullptr;
+  if (h->profiling) {
+    const int64_t words = (int64_t)grid * kProfPhases * 2;
+    if ((st = h->prof.ensure(words))) return st;
+    if (h->prof_grid != grid) {  // timers accumulate over solves of one grid size
+      if (cudaMemsetAsync(h->prof.p, 0, sizeof(unsigned long long) * words, s) != cudaSuccess)
+        return CUP2D_CUDA_ERROR;
+      h->prof_grid = grid;
+    }
+    prof = h->prof.p;
+  }
   if (stats) cudaEventRecord(h->ev0, s);
   cudaError_t e;
   if (o.precision == CUP2D_PREC_MIXED) {
@@ -408,6 +467,8 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.max_iter = o.max_iter;
     a.subtract_mean = o.subtract_mean;
     a.timeout_ns = tns;
+    a.prof = prof;
+    a.sbounds = h->sbounds.p;
     e = launch_bicgstab_mixed(a, grid, s);
   } else {
     SolveArgs64 a{};
@@ -432,6 +493,8 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.max_iter = o.max_iter;
     a.subtract_mean = o.subtract_mean;
     a.timeout_ns = tns;
+    a.prof = prof;
+    a.sbounds = h->sbounds.p;
     e = launch_bicgstab64(a, grid, s);
   }
   if (e != cudaSuccess) return from_cuda(e);
@@ -468,20 +531,44 @@ int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x, cup2d_solv
 
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream) {
   if (!h || !d_x || !d_y) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, s));
 }
 
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream) {
   if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   return from_cuda(launch_precond64(h->P.p, h->nb, d_p, d_z, s));
 }
 
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream) {
   if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   return from_cuda(launch_precond32(h->P32.p, h->nb, d_p, d_z, s));
+}
+
+int cup2d_poisson_set_profiling(cup2d_poisson* h, int32_t enable) {
+  if (!h) return CUP2D_INVALID_ARGUMENT;
+  h->profiling = enable != 0;
+  h->prof_grid = 0;  // next profiled solve starts from zero
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_profile(cup2d_poisson* h, double* compute_ms, double* wait_ms, int32_t nphases) {
+  if (!h || !compute_ms || !wait_ms || nphases < kProfPhases) return CUP2D_INVALID_ARGUMENT;
+  for (int q = 0; q < kProfPhases; ++q) compute_ms[q] = wait_ms[q] = 0.0;
+  if (!h->profiling || h->prof_grid <= 0) return CUP2D_OK;
+  const int g = h->prof_grid;
+  std::vector<unsigned long long> t((size_t)g * kProfPhases * 2);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+      cudaMemcpy(t.data(), h->prof.p, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  for (int c = 0; c < g; ++c)
+    for (int q = 0; q < kProfPhases; ++q) {
+      compute_ms[q] += 1e-6 * (double)t[((size_t)c * kProfPhases + q) * 2] / g;
+      wait_ms[q] += 1e-6 * (double)t[((size_t)c * kProfPhases + q) * 2 + 1] / g;
+    }
+  return CUP2D_OK;
 }
 
 int cup2d_poisson_explicit_info(cup2d_poisson* h, int64_t* rows, int64_t* nnz) {

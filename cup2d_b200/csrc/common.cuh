@@ -31,8 +31,14 @@ struct MeshView {
   const int32_t* __restrict__ xcol;
   const double* __restrict__ xval;
   const float* __restrict__ xval32;
-  const double* __restrict__ hblk;  // cell size per block
+  const double* __restrict__ hblk;     // cell size per block
+  const int32_t* __restrict__ rowcell; // [R] cell index of each explicit row
+  const int32_t* __restrict__ wprefix; // [nb+1] prefix sum of SpMV cost weights
 };
+
+// SpMV cost weight of a block: its 64 stencil rows count as kSpmvBlockCost,
+// each explicit (coarse/fine) row adds one.
+constexpr int32_t kSpmvBlockCost = 32;
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -62,18 +68,29 @@ __device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
 // another CTA raised `abort_flag`, the CTA raises the flag itself and the
 // barrier returns false; callers then leave the kernel.  Every thread of the
 // CTA must call it (it contains __syncthreads).
+//
+// Profiling (the device-side counterpart of CUP2D's DeviceProfiler regions,
+// source/Utils/DeviceProfiler.cuh): when `prof` is set, thread 0 adds to
+// prof[(cta*kProfPhases + phase)*2 + {0,1}] the ns spent computing the phase
+// that ends at this barrier and the ns spent waiting in it.
+constexpr int kProfPhases = 10;
+
 struct GridBarrier {
   unsigned* counter;
   int* abort_flag;
   unsigned nparties;
   unsigned long long deadline_ns;
   unsigned epoch;  // barriers passed so far by this CTA
+  unsigned long long* prof;
+  unsigned long long last;  // thread 0: when it left the previous barrier
 
-  __device__ __forceinline__ bool sync(int* smem_flag) {
+  __device__ __forceinline__ bool sync(int* smem_flag, int phase = 0) {
     __syncthreads();
     ++epoch;
     if (threadIdx.x == 0) {
       int ok = 1;
+      unsigned long long t_arrive = 0;
+      if (prof) t_arrive = globaltimer_ns();
       __threadfence();
       red_release_add_u32(counter, 1u);
       const unsigned target = epoch * nparties;
@@ -89,6 +106,13 @@ struct GridBarrier {
         if (spins > 256) __nanosleep(64);
       }
       __threadfence();
+      if (prof) {
+        const unsigned long long t_depart = globaltimer_ns();
+        unsigned long long* p = prof + ((size_t)blockIdx.x * kProfPhases + phase) * 2;
+        p[0] += t_arrive - last;
+        p[1] += t_depart - t_arrive;
+        last = t_depart;
+      }
       *smem_flag = ok;
     }
     __syncthreads();

@@ -32,7 +32,10 @@ struct DeviceMesh {
   int32_t* scan_tmp = nullptr;
   int* err = nullptr;
   int64_t R = 0, nnz = 0;
+  int32_t* wcost = nullptr;       // [nb] SpMV cost weights
+  int32_t* wprefix = nullptr;     // [nb+1]
   int32_t* rowlen = nullptr;      // [R]
+  int32_t* rowcell = nullptr;     // [R]
   int32_t* xptr = nullptr;        // [R+1]
   int32_t* xcol = nullptr;        // [nnz]
   double* xval = nullptr;         // [nnz]
@@ -51,6 +54,8 @@ struct DeviceMesh {
     v.xcol = xcol;
     v.xval = xval;
     v.xval32 = xval32;
+    v.rowcell = rowcell;
+    v.wprefix = wprefix;
     v.hblk = hblk;
     return v;
   }
@@ -98,6 +103,8 @@ struct SolveArgs64 {
   double tol_abs, tol_rel;
   int max_restarts, max_iter, subtract_mean;
   unsigned long long timeout_ns;
+  unsigned long long* prof;  // per-CTA phase timers, or null
+  const int32_t* sbounds;    // [grid+1] SpMV block ranges, balanced by cost
 };
 
 // Mixed precision: FP32 Krylov vectors, FP64 solution and true residual.
@@ -120,9 +127,12 @@ struct SolveArgsMixed {
   double tol_abs, tol_rel, reliable_delta;
   int max_restarts, max_iter, subtract_mean, reliable_restart;
   unsigned long long timeout_ns;
+  unsigned long long* prof;  // per-CTA phase timers, or null
+  const int32_t* sbounds;    // [grid+1] SpMV block ranges, balanced by cost
 };
 
 constexpr int kSolveThreads = 256;
+constexpr int kSolveCtasPerSm = 3;
 
 // Largest co-resident grid of the persistent kernels on this device.
 int max_coop_grid_fp64(int device);

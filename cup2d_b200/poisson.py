@@ -35,7 +35,7 @@ def default_opts() -> L.SolveOpts:
 
 
 def make_opts(tol_abs=0.0, tol_rel=1e-8, max_restarts=100, max_iter=1000, precision="fp64",
-              subtract_mean=True, reliable_delta=0.1, reliable_restart=True, timeout_ms=20000) -> L.SolveOpts:
+              subtract_mean=True, reliable_delta=0.5, reliable_restart=True, timeout_ms=20000) -> L.SolveOpts:
     o = default_opts()
     o.tol_abs = tol_abs
     o.tol_rel = tol_rel
@@ -96,10 +96,19 @@ class Solver:
         L.check(L.lib().cup2d_poisson_set_grid(self._h, int(grid)), "cup2d_poisson_set_grid")
 
     # ------------------------------------------------------------ solve ---
-    def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None) -> np.ndarray:
-        """Host arrays in, host array out (copies inside the call)."""
+    def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Host arrays in, host array out (the host<->device copies are part
+        of the call).  With `out` (contiguous float64, e.g. pinned memory) the
+        initial guess is read from and the solution written to that array."""
         b = np.ascontiguousarray(b, dtype=np.float64)
-        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != b.shape:
+                raise ValueError("out must be a contiguous float64 array shaped like b")
+            x = out
+            if x0 is not None:
+                x[...] = x0
+        else:
+            x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
         st = L.SolveStats()
         L.check(L.lib().cup2d_poisson_solve(self._h, _pd(b), _pd(x), C.byref(st)), "cup2d_poisson_solve")
         self.last_stats = st.as_dict()
@@ -111,7 +120,7 @@ class Solver:
         _check_dev(b, self.ncells)
         _check_dev(x, self.ncells)
         st = L.SolveStats()
-        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        s = _stream_handle(stream)
         L.check(L.lib().cup2d_poisson_solve_device(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
                                                    C.byref(st) if stats else None, s),
                 "cup2d_poisson_solve_device")
@@ -124,13 +133,13 @@ class Solver:
     def apply(self, x, y, stream=None) -> None:
         _check_dev(x, self.ncells)
         _check_dev(y, self.ncells)
-        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        s = _stream_handle(stream)
         L.check(L.lib().cup2d_poisson_apply(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s),
                 "cup2d_poisson_apply")
 
     def precond(self, p, z, stream=None) -> None:
         fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond
-        s = C.c_void_p(stream.cuda_stream if stream is not None else 0)
+        s = _stream_handle(stream)
         L.check(fn(self._h, C.c_void_p(p.data_ptr()), C.c_void_p(z.data_ptr()), s), "cup2d_poisson_precond")
 
     def export_csr(self):
@@ -147,11 +156,33 @@ class Solver:
                 "cup2d_poisson_export_csr")
         return rp, col, val
 
+    PHASES = ("residual/init", "A: p, P^-1", "B: SpMV (rhat,nu)", "C: x, s, P^-1", "D: SpMV (t,s),(t,t)",
+              "E: x, r, norms", "true residual", "mean removal", "sum b", "unused")
+
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(L.lib().cup2d_poisson_set_profiling(self._h, int(bool(enable))), "set_profiling")
+
+    def profile(self) -> dict:
+        """Per-phase (compute ms, barrier-wait ms), per-CTA averages since
+        profiling was enabled."""
+        c = np.zeros(10)
+        w = np.zeros(10)
+        L.check(L.lib().cup2d_poisson_profile(self._h, _pd(c), _pd(w), 10), "profile")
+        return {name: (float(c[i]), float(w[i])) for i, name in enumerate(self.PHASES) if c[i] or w[i]}
+
     def explicit_info(self) -> tuple[int, int]:
         r = C.c_int64()
         z = C.c_int64()
         L.check(L.lib().cup2d_poisson_explicit_info(self._h, C.byref(r), C.byref(z)), "explicit_info")
         return r.value, z.value
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    """cudaStream_t of a torch stream; torch's current stream by default."""
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
 
 
 def _check_dev(t, n: int) -> None:

@@ -20,8 +20,9 @@
  *   - Every entry point returns a cup2d_status; none exits or aborts.
  *   - A handle is not thread-safe; it runs its work on one CUDA stream.
  *   - Pointers named d_* are device pointers on the handle's device; the
- *     others are host pointers.  `stream` is a cudaStream_t (NULL = the
- *     handle's own stream).
+ *     others are host pointers.  `stream` is a cudaStream_t used as given
+ *     (NULL is the legacy default stream, as in the CUDA runtime).  The
+ *     host-buffer solve runs on the handle's own stream.
  */
 #ifndef CUP2D_POISSON_H
 #define CUP2D_POISSON_H
@@ -136,6 +137,17 @@ int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void
  * get n and nnz. */
 int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n, int64_t* nnz,
                              int64_t* row_ptr, int32_t* col, double* val);
+/* Per-phase device timers (the counterpart of DeviceProfiler,
+ * source/Utils/DeviceProfiler.cuh:26-108, compiled in with -DBICGSTAB_PROFILER
+ * in the reference; here switched at run time).  While enabled, every solve
+ * adds, per CTA, the time spent computing each phase and waiting at the grid
+ * barrier that ends it.  cup2d_poisson_profile returns the per-CTA averages
+ * in ms accumulated since enabling, for phases 0 residual / mean, 1 pass A
+ * (p, P^-1), 2 pass B (SpMV), 3 pass C (x, s, P^-1), 4 pass D (SpMV),
+ * 5 pass E (x, r, norms), 6 true-residual refresh, 7 mean removal, 8 sum b;
+ * nphases >= 10. */
+int cup2d_poisson_set_profiling(cup2d_poisson* h, int32_t enable);
+int cup2d_poisson_profile(cup2d_poisson* h, double* compute_ms, double* wait_ms, int32_t nphases);
 /* Explicit (coarse/fine) rows only: number of rows and non-zeros. */
 int cup2d_poisson_explicit_info(cup2d_poisson* h, int64_t* rows, int64_t* nnz);
 
