@@ -318,6 +318,37 @@ def run_reference(args, world, rank) -> dict | None:
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def profile_case(args) -> int:
+    """Short solves for profilers: two FP64 and two mixed solves of the
+    workload, each capped at `--profile-iters` iterations, one kernel launch
+    each.  Prints the solve statistics; no timing is reported."""
+    import torch
+
+    from cup2d_b200 import Solver
+    from cup2d_b200.problems import large_mesh, small_mesh
+    dev = torch.device("cuda", 0)
+    mesh = large_mesh() if args.workload == "large" else small_mesh()
+    b = torch.from_numpy(mesh.rhs_fourier(17)).to(dev)
+    it = args.profile_iters
+    with Solver(mesh, tol_rel=0.0, max_iter=it) as s:
+        for prec in ("fp64", "mixed"):
+            s.set_opts(tol_rel=0.0, max_iter=it, precision=prec)
+            for _ in range(2):
+                x = torch.zeros(mesh.ncells, dtype=torch.float64, device=dev)
+                print(prec, s.solve_device(b, x), flush=True)
+            if args.phases:
+                # one more solve with the device phase timers on
+                s.set_profiling(True)
+                x = torch.zeros(mesh.ncells, dtype=torch.float64, device=dev)
+                st = s.solve_device(b, x)
+                n = max(1, st["iterations"])
+                print(f"{prec}: {st['solve_ms'] * 1e3 / n:.2f} us/iteration over {n} iterations", flush=True)
+                for name, (c, w) in s.profile().items():
+                    print(f"  {name:22s} compute {c * 1e3 / n:7.2f} us/it   barrier wait {w * 1e3 / n:7.2f} us/it")
+                s.set_profiling(False)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -326,7 +357,12 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["large", "small"], default="large")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile-iters", type=int, default=0,
+                    help="profiling case: capped solves only (see profile_case)")
+    ap.add_argument("--phases", action="store_true", help="with --profile-iters: print device phase timers")
     args = ap.parse_args(argv)
+    if args.profile_iters > 0:
+        return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":

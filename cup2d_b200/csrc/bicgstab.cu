@@ -32,10 +32,12 @@
 // solves cannot refine.  Instead x stays FP64 and is updated in passes C and
 // E from the FP32 z; only the Krylov vectors (r, rhat, p, nu, t, z) are
 // FP32.  When the FP32 residual has dropped by `reliable_delta` since its
-// last replacement, or claims convergence, it is replaced by the true
-// residual b - A x computed in FP64 (with b projected to zero sum, the
-// Neumann compatibility condition), without restarting the recurrences.
-// Convergence is declared only on the true FP64 residual.
+// last replacement, claims convergence, or a sweep stalls, it is replaced by
+// the true residual b - A x computed in FP64 (with b projected to zero sum,
+// the Neumann compatibility condition); by default the recurrences restart
+// from it (rhat = r, p = nu = 0), which FP32 needs here: on the large
+// meshes the unrestarted FP32 recurrences diverge.  Convergence is declared
+// only on the true FP64 residual.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
