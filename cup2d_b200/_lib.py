@@ -57,6 +57,8 @@ SIGNATURES = {
     "cup2d_poisson_solve": (C.c_int, [C.c_void_p, P_f64, P_f64, C.POINTER(SolveStats)]),
     "cup2d_poisson_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.POINTER(SolveStats), C.c_void_p]),
+    "cup2d_poisson_solve_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                     C.POINTER(SolveStats), C.c_void_p]),
     "cup2d_poisson_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

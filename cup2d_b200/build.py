@@ -17,8 +17,8 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libcup2d_poisson.so"
 
-SOURCES = ["assemble.cu", "bicgstab.cu", "capi.cu", "problems.cpp", "forest.cpp"]
-HEADERS = ["common.cuh", "kernels.hpp", "spmv.cuh", "forest.hpp"]
+SOURCES = ["assemble.cu", "bicgstab.cu", "capi.cu", "noalloc.cu", "problems.cpp", "forest.cpp"]
+HEADERS = ["common.cuh", "kernels.hpp", "spmv.cuh", "handle_view.hpp", "forest.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",

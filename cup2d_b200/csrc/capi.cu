@@ -19,6 +19,7 @@
 
 #include "../../include/cup2d_poisson.h"
 #include "forest.hpp"
+#include "handle_view.hpp"
 #include "kernels.hpp"
 
 using namespace cup2d;
@@ -649,3 +650,21 @@ int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n_out, int64_t* nnz_out,
 }
 
 }  // extern "C"
+
+namespace cup2d {
+
+int handle_view(const cup2d_poisson* h, HandleView* out) {
+  if (!h || !out || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  out->device = h->device;
+  out->M = h->mesh.view();
+  out->P = h->P.p;
+  out->nb = h->nb;
+  out->grid = h->grid_for(h->grid64);
+  out->opts = h->opts;
+  out->wprefix = &h->wprefix_host;
+  out->ev0 = h->ev0;
+  out->ev1 = h->ev1;
+  return CUP2D_OK;
+}
+
+}  // namespace cup2d

@@ -1,0 +1,170 @@
+// FP64 solve that allocates no device memory.
+//
+// cup2d_poisson_solve_device allocates its Krylov vectors and reduction
+// scratch through the handle the first time they are needed.  Some callers
+// must not allocate device memory at solve time: an application whose device
+// memory is owned by its own pool allocator (the rest of the GPU is already
+// claimed), or a time-step loop that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree can cause.  This entry point runs the
+// same FP64 persistent kernel (k_bicgstab64) with all of its scratch (seven
+// Krylov vectors, per-CTA reduction partials, the grid-barrier counter, the
+// abort flag, the SpMV block ranges and the statistics) in one file-scope
+// static device array, so the call itself allocates nothing: no cudaMalloc,
+// no cudaFree, no allocating library routine.
+//
+// Limits and rules (also in include/cup2d_poisson.h):
+//  * at most kNoAllocMaxBlocks = 4096 blocks (262,144 cells) and 1024 CTAs;
+//    larger problems are rejected with CUP2D_INVALID_ARGUMENT;
+//  * the array is 14.2 MiB of static device memory that every GPU which
+//    loads the library holds until the process exits;
+//  * all calls share the array, which keeps the last call's contents; calls
+//    whose work overlaps on the GPU (other streams, other threads) race, so
+//    callers serialise them;
+//  * the first call on a device looks up the array's device address with
+//    cudaGetSymbolAddress (with that device current) and caches it; make
+//    that first call before any stream capture.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/cup2d_poisson.h"
+#include "handle_view.hpp"
+#include "kernels.hpp"
+
+namespace cup2d {
+namespace {
+
+constexpr int64_t kNoAllocMaxBlocks = CUP2D_NOALLOC_MAX_BLOCKS;
+constexpr int64_t kNoAllocMaxCells = kNoAllocMaxBlocks * kBLEN;
+constexpr int kNoAllocMaxGrid = 1024;
+constexpr int kMaxDevices = 64;
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Scratch layout (byte offsets, 256-byte aligned)
+constexpr size_t kVecBytes = align256(sizeof(double) * kNoAllocMaxCells);
+constexpr size_t kOffVec = 0;  // xo, r, rh, p, nu, t, z
+constexpr size_t kOffRed = kOffVec + 7 * kVecBytes;
+constexpr size_t kOffBounds = kOffRed + align256(sizeof(double) * kRedQ * kNoAllocMaxGrid);
+constexpr size_t kOffBar = kOffBounds + align256(sizeof(int32_t) * (kNoAllocMaxGrid + 1));
+constexpr size_t kOffAbort = kOffBar + 256;
+constexpr size_t kOffStats = kOffAbort + 256;
+constexpr size_t kScratchBytes = kOffStats + align256(sizeof(DevStats));
+
+}  // namespace
+}  // namespace cup2d
+
+// The scratch of every call of cup2d_poisson_solve_device_noalloc.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[cup2d::kScratchBytes];
+
+namespace cup2d {
+namespace {
+
+std::mutex g_scratch_mu;
+char* g_scratch_base[kMaxDevices] = {};
+
+// Device address of the scratch on the current device (looked up once).
+int scratch_base(int device, char** out) {
+  if (device < 0 || device >= kMaxDevices) return CUP2D_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_base[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return CUP2D_CUDA_ERROR;
+    }
+    g_scratch_base[device] = static_cast<char*>(p);
+  }
+  *out = g_scratch_base[device];
+  return CUP2D_OK;
+}
+
+}  // namespace
+}  // namespace cup2d
+
+extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, double* d_x,
+                                                  cup2d_solve_stats* stats, void* stream) {
+  using namespace cup2d;
+  if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  HandleView v;
+  if (handle_view(h, &v) != CUP2D_OK) return CUP2D_INVALID_ARGUMENT;
+  if (v.nb > kNoAllocMaxBlocks) return CUP2D_INVALID_ARGUMENT;  // beyond the static scratch
+  int current = -1;
+  if (cudaGetDevice(&current) != cudaSuccess || current != v.device) return CUP2D_INVALID_ARGUMENT;
+  char* base = nullptr;
+  int st = scratch_base(current, &base);
+  if (st != CUP2D_OK) return st;
+  const cup2d_solve_opts& o = v.opts;
+  const int grid = std::max(1, std::min(v.grid, kNoAllocMaxGrid));
+  const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
+  if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  // SpMV block ranges balanced by cost (same rule as the allocating path),
+  // staged from the stack; a pageable source is copied before the call returns
+  int32_t bounds[kNoAllocMaxGrid + 1];
+  const std::vector<int32_t>& wp = *v.wprefix;
+  const int64_t W = wp.back();
+  for (int c = 0; c <= grid; ++c)
+    bounds[c] = (int32_t)(std::lower_bound(wp.begin(), wp.end(), (int32_t)(W * c / grid)) - wp.begin());
+  bounds[grid] = (int32_t)v.nb;
+  if (cudaMemcpyAsync(base + kOffBounds, bounds, sizeof(int32_t) * (grid + 1), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemsetAsync(base + kOffBar, 0, 256, s) != cudaSuccess ||       // barrier counter starts at 0
+      cudaMemsetAsync(base + kOffAbort, 0, 256, s) != cudaSuccess)       // abort flag starts clear
+    return CUP2D_CUDA_ERROR;
+
+  double* vec = reinterpret_cast<double*>(base + kOffVec);
+  const size_t stride = kVecBytes / sizeof(double);
+  SolveArgs64 a{};
+  a.M = v.M;
+  a.P = v.P;
+  a.b = d_b;
+  a.x = d_x;
+  a.xo = vec + 0 * stride;
+  a.r = vec + 1 * stride;
+  a.rh = vec + 2 * stride;
+  a.p = vec + 3 * stride;
+  a.nu = vec + 4 * stride;
+  a.t = vec + 5 * stride;
+  a.z = vec + 6 * stride;
+  a.red = reinterpret_cast<double*>(base + kOffRed);
+  a.bar = reinterpret_cast<unsigned*>(base + kOffBar);
+  a.abort_flag = reinterpret_cast<int*>(base + kOffAbort);
+  a.stats = reinterpret_cast<DevStats*>(base + kOffStats);
+  a.tol_abs = o.tol_abs;
+  a.tol_rel = o.tol_rel;
+  a.max_restarts = o.max_restarts;
+  a.max_iter = o.max_iter;
+  a.subtract_mean = o.subtract_mean;
+  a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
+  a.prof = nullptr;
+  a.sbounds = reinterpret_cast<const int32_t*>(base + kOffBounds);
+
+  if (stats) cudaEventRecord(v.ev0, s);
+  const cudaError_t e = launch_bicgstab64(a, grid, s);
+  if (e != cudaSuccess) return e == cudaErrorNoDevice ? CUP2D_NO_DEVICE : CUP2D_CUDA_ERROR;
+  if (!stats) return CUP2D_OK;
+  cudaEventRecord(v.ev1, s);
+  DevStats ds;
+  int aborted = 0;
+  if (cudaMemcpyAsync(&ds, base + kOffStats, sizeof(DevStats), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&aborted, base + kOffAbort, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, v.ev0, v.ev1);
+  stats->status = aborted ? CUP2D_TIMEOUT : ds.status;
+  stats->iterations = ds.iterations;
+  stats->restarts = ds.restarts;
+  stats->refinements = 0;
+  stats->err_init = ds.err_init;
+  stats->err_final = ds.err_opt;
+  stats->rel_res_inf = ds.err_init > 0 ? ds.err_opt / ds.err_init : 0.0;
+  stats->solve_ms = ms;
+  return aborted ? CUP2D_TIMEOUT : CUP2D_OK;
+}

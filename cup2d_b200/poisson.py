@@ -129,6 +129,23 @@ class Solver:
             return self.last_stats
         return None
 
+    def solve_device_noalloc(self, b, x, stream=None) -> dict:
+        """The FP64 device solve without any device allocation, for callers
+        that must not allocate at solve time (their device memory belongs to
+        their own pool, or their loop cannot afford the synchronisation an
+        allocation can cause).  Scratch lives in one static 14.2 MiB device
+        array shared by all calls: at most CUP2D_NOALLOC_MAX_BLOCKS (4096)
+        blocks, and calls that overlap on the GPU race."""
+        _check_dev(b, self.ncells)
+        _check_dev(x, self.ncells)
+        st = L.SolveStats()
+        L.check(L.lib().cup2d_poisson_solve_device_noalloc(self._h, C.c_void_p(b.data_ptr()),
+                                                           C.c_void_p(x.data_ptr()), C.byref(st),
+                                                           _stream_handle(stream)),
+                "cup2d_poisson_solve_device_noalloc")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
     # ------------------------------------------------------ components ---
     def apply(self, x, y, stream=None) -> None:
         _check_dev(x, self.ncells)

@@ -128,6 +128,24 @@ int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x,
 int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
                                cup2d_solve_stats* stats, void* stream);
 
+/* The FP64 device solve without any device allocation.  This entry point has
+ * no counterpart in the reference.  It is for callers that must not allocate
+ * device memory when they solve: an application whose device memory belongs
+ * to its own pool allocator, or a time-step loop that cannot afford the
+ * device-wide synchronisation cudaMalloc/cudaFree can cause.  The handle's
+ * operator (built at create/update time) and the caller's b and x are the
+ * inputs and outputs; every scratch buffer of the solve lives in one static
+ * device array of 14.2 MiB that each GPU loading the library holds until
+ * exit.  Limits: at most CUP2D_NOALLOC_MAX_BLOCKS blocks (larger problems
+ * return CUP2D_INVALID_ARGUMENT) and always the plain FP64 form.  All calls
+ * share the array: calls whose GPU work overlaps race, so serialise them.
+ * The first call on a device looks up the array's address (the handle's
+ * device must be current); make it before any stream capture.  Otherwise
+ * behaves as cup2d_poisson_solve_device. */
+#define CUP2D_NOALLOC_MAX_BLOCKS 4096
+int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, double* d_x,
+                                       cup2d_solve_stats* stats, void* stream);
+
 /* Building blocks (device buffers), exposed for parity tests. */
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream);
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
