@@ -228,12 +228,16 @@ def run_ours(args, world, rank, local) -> dict | None:
     def pct(v, q):
         return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
 
-    traffic = None
+    # DRAM bytes per launch: the per-iteration traffic of one ncu capture of
+    # this workload (profiles/traffic.json) times this run's iterations
+    traffic = traffic_d = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
         tj = json.loads(tp.read_text()).get(args.workload, {})
         if "dram_bytes_per_iteration_mixed" in tj:
             traffic = tj["dram_bytes_per_iteration_mixed"] * (sum(it_m) / K)
+        if "dram_bytes_per_iteration_fp64" in tj:
+            traffic_d = tj["dram_bytes_per_iteration_fp64"] * (sum(it_d) / K)
     value = world * K / (tot_mixed * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -249,7 +253,8 @@ def run_ours(args, world, rank, local) -> dict | None:
                        "latency_ms": {"p50": pct(latd, 0.5), "p99": pct(latd, 0.99)},
                        "iterations_mean": statistics.mean(it_d),
                        "roofline": {"bound": "hbm", "achieved": ach_d, "peak": peak, "unit": "GB/s",
-                                    "frac": ach_d / peak}},
+                                    "frac": ach_d / peak, "traffic": traffic_d,
+                                    "kernel": "k_bicgstab64 (one persistent launch per solve)"}},
         "speedup_mixed_vs_fp64": tot_fp64 / tot_mixed,
         "roofline": {"bound": "hbm", "achieved": ach_m, "peak": peak, "unit": "GB/s", "frac": ach_m / peak,
                      "traffic": traffic, "kernel": "k_bicgstab_mixed (one persistent launch per solve)",

@@ -66,6 +66,15 @@ SIGNATURES = {
     "cup2d_poisson_explicit_info": (C.c_int, [C.c_void_p, P_i64, P_i64]),
     "cup2d_poisson_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "cup2d_poisson_profile": (C.c_int, [C.c_void_p, P_f64, P_f64, C.c_int32]),
+    "cup2d_batch_create": (C.c_int, [C.c_int32, C.POINTER(Forest), C.POINTER(SolveOpts),
+                                     C.POINTER(C.c_void_p)]),
+    "cup2d_batch_set_opts": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts)]),
+    "cup2d_batch_set_team": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cup2d_batch_size": (C.c_int32, [C.c_void_p]),
+    "cup2d_batch_num_cells": (C.c_int64, [C.c_void_p, C.c_int32]),
+    "cup2d_batch_solve_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                           C.POINTER(SolveStats), C.c_void_p]),
+    "cup2d_batch_destroy": (C.c_int, [C.c_void_p]),
     "cup2d_mesh_disks": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                    C.c_int32, P_f64, C.c_double, C.POINTER(C.c_void_p)]),
     "cup2d_mesh_uniform": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,

@@ -40,6 +40,8 @@
 // only on the true FP64 residual.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.hpp"
 #include "spmv.cuh"
@@ -78,6 +80,11 @@ struct Smem {
   double wred[kWarps][6];
   double gres[6];
   int flag;
+  // the CTAs solving one problem together: this CTA's rank among them and
+  // their number (the whole grid for a single solve, a group in a batch)
+  int team_rank, team_size;
+  int64_t bounds[2];  // batch: this CTA's SpMV block range of the current problem
+  int slot;           // batch: the problem the team works on
 };
 
 // max that propagates NaN (fmax drops it, which would let a blown-up
@@ -105,7 +112,7 @@ __device__ __forceinline__ void cta_partials(Smem& sm, const double (&v)[NV], un
     double acc = sm.wred[0][q];
     for (int k = 1; k < kWarps; ++k)
       acc = ((is_max >> q) & 1u) ? nanmax(acc, sm.wred[k][q]) : acc + sm.wred[k][q];
-    red[(q0 + q) * gridDim.x + blockIdx.x] = acc;
+    red[(q0 + q) * sm.team_size + sm.team_rank] = acc;
   }
 }
 
@@ -114,9 +121,9 @@ __device__ __forceinline__ void grid_reduce(Smem& sm, unsigned is_max, const dou
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (w < NV) {
     const bool mx = (is_max >> w) & 1u;
-    const double* src = red + (q0 + w) * gridDim.x;
+    const double* src = red + (q0 + w) * sm.team_size;
     double acc = 0.0;
-    for (unsigned j = lane; j < gridDim.x; j += 32) {
+    for (int j = lane; j < sm.team_size; j += 32) {
       const double v = __ldcg(src + j);
       acc = mx ? nanmax(acc, v) : acc + v;
     }
@@ -567,25 +574,29 @@ __device__ __forceinline__ void take_best(bool best_is_x, double* __restrict__ x
   }
 }
 
-}  // namespace
+// ============================================ one problem, one team ========
 
-// ====================================================== plain FP64 ========
+__device__ __forceinline__ void write_stats(const Smem& sm, DevStats* stats, const IterState& st, int refinements,
+                                            double err_final, double norm_ax0) {
+  if (sm.team_rank == 0 && threadIdx.x == 0) {
+    stats->status = st.status;
+    stats->iterations = st.iters;
+    stats->restarts = st.restarts;
+    stats->refinements = refinements;
+    stats->err_init = st.err_init;
+    stats->err_opt = err_final;
+    stats->norm_ax0 = norm_ax0;
+  }
+}
 
-// Three CTAs per SM (80 registers): the passes are bound by per-warp memory
-// latency, and the extra warps outweigh the spills this costs (measured on
-// the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(SolveArgs64 S) {
-  __shared__ Smem sm;
-  const int64_t nb = S.M.nb;
-  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
-  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
-  Pinv<double> pin;
-  pin.load(sm.P, S.P, nullptr);
-  __syncthreads();
-  const MeshView& M = S.M;
-  const Vecs<double, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
-
+// Plain FP64 solve of one problem by the team: BiCGSTABSolver::main
+// (BiCGSTAB.cu:412-620) and the mean removal (ExpAMRSolver.cpp:383-415).
+// [b0,b1) is this CTA's block range, [sb0,sb1) its SpMV range.
+__device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
+                           const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
+                           int64_t sb1) {
+  const MeshView& M = pr.M;
+  const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z};
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
   {
     struct Epi {
@@ -601,12 +612,12 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
         v[1] = nanmax(v[1], fabs(rv));
         v[2] += rv * rv;
       }
-    } epi{S.b, S.r, S.rh, {0.0, 0.0, 0.0}};
-    spmv_range<double>(M, S.x, sb0, sb1, epi);
-    cta_partials<3>(sm, epi.v, 0x3u, S.red, Q_INIT);
+    } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
+    spmv_range<double>(M, pr.x, sb0, sb1, epi);
+    cta_partials<3>(sm, epi.v, 0x3u, red, Q_INIT);
   }
-  if (!B.sync(&sm.flag, 0)) return;
-  grid_reduce<3>(sm, 0x3u, S.red, Q_INIT);
+  if (!B.sync(&sm.flag, 0)) return false;
+  grid_reduce<3>(sm, 0x3u, red, Q_INIT);
   IterState st;
   const double norm_ax0 = sm.gres[0];
   st.err_init = sm.gres[1];
@@ -619,57 +630,42 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
   const MixedCtx none{};
-  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, S.red, b0, b1, sb0, sb1, S.tol_abs, S.tol_rel,
-                                            S.max_restarts, S.max_iter, none, st))
-    return;
-  take_best(st.best_is_x, S.x, S.xo, b0, b1);
-  if (S.subtract_mean && !subtract_mean(sm, B, M, S.x, S.red, b0, b1)) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    S.stats->status = st.status;
-    S.stats->iterations = st.iters;
-    S.stats->restarts = st.restarts;
-    S.stats->refinements = 0;
-    S.stats->err_init = st.err_init;
-    S.stats->err_opt = st.err_opt;
-    S.stats->norm_ax0 = norm_ax0;
-  }
+  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, red, b0, b1, sb0, sb1, sp.tol_abs, sp.tol_rel,
+                                            sp.max_restarts, sp.max_iter, none, st))
+    return false;
+  take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
+  if (sp.subtract_mean && !subtract_mean(sm, B, M, pr.x, red, b0, b1)) return false;
+  write_stats(sm, pr.stats, st, 0, st.err_opt, norm_ax0);
+  return true;
 }
 
-// ================================================ mixed precision =========
-
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
-  __shared__ Smem sm;
+// Mixed-precision solve of one problem by the team.
+__device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, const ProblemMixed& pr,
+                            const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
+                            int64_t sb1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t nb = S.M.nb;
-  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
-  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
-  Pinv<float> pin;
-  pin.load(sm.P, nullptr, S.P32);
-  __syncthreads();
-  const Vecs<float, double> V{S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z};
-
+  const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z};
   // Neumann compatibility: project b to zero sum (sum b / n)
   {
     double v[1] = {0.0};
     for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
       const int64_t o = blk * kBLEN;
-      v[0] += __ldg(S.b + o + lane) + __ldg(S.b + o + lane + 32);
+      v[0] += __ldg(pr.b + o + lane) + __ldg(pr.b + o + lane + 32);
     }
-    cta_partials<1>(sm, v, 0u, S.red, Q_SUMB);
+    cta_partials<1>(sm, v, 0u, red, Q_SUMB);
   }
-  if (!B.sync(&sm.flag, 8)) return;
-  grid_reduce<1>(sm, 0u, S.red, Q_SUMB);
+  if (!B.sync(&sm.flag, 8)) return false;
+  grid_reduce<1>(sm, 0u, red, Q_SUMB);
   MixedCtx mx;
-  mx.b = S.b;
-  mx.mean_b = sm.gres[0] / (double)(nb * kBLEN);
-  mx.delta = S.reliable_delta;
-  mx.tol_abs = S.tol_abs;
-  mx.tol_rel = S.tol_rel;
-  mx.restart = S.reliable_restart != 0;
-  true_residual(sm, S.M, S.b, mx.mean_b, S.x, S.r, S.rh, true, S.red, sb0, sb1);
-  if (!B.sync(&sm.flag, 0)) return;
-  grid_reduce<5>(sm, 0x11u, S.red, Q_RU);
+  mx.b = pr.b;
+  mx.mean_b = sm.gres[0] / (double)(pr.M.nb * kBLEN);
+  mx.delta = sp.reliable_delta;
+  mx.tol_abs = sp.tol_abs;
+  mx.tol_rel = sp.tol_rel;
+  mx.restart = sp.reliable_restart != 0;
+  true_residual(sm, pr.M, pr.b, mx.mean_b, pr.x, pr.r, pr.rh, true, red, sb0, sb1);
+  if (!B.sync(&sm.flag, 0)) return false;
+  grid_reduce<5>(sm, 0x11u, red, Q_RU);
   IterState st;
   st.err_init = sm.gres[0];
   st.err_true = sm.gres[0];
@@ -682,24 +678,136 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   st.updates = 0;
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
-  const bool done0 = st.err_true <= S.tol_abs || st.err_true == 0.0;
+  const bool done0 = st.err_true <= sp.tol_abs || st.err_true == 0.0;
   if (done0) {
     st.status = CUP2D_OK;
-  } else if (!bicgstab_loop<float, double, true>(sm, B, S.M, pin, V, S.red, b0, b1, sb0, sb1, S.tol_abs, S.tol_rel,
-                                                 S.max_restarts, S.max_iter, mx, st)) {
-    return;
+  } else if (!bicgstab_loop<float, double, true>(sm, B, pr.M, pin, V, red, b0, b1, sb0, sb1, sp.tol_abs,
+                                                 sp.tol_rel, sp.max_restarts, sp.max_iter, mx, st)) {
+    return false;
   }
-  take_best(st.best_is_x, S.x, S.xo, b0, b1);
-  if (S.subtract_mean && !subtract_mean(sm, B, S.M, S.x, S.red, b0, b1)) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    S.stats->status = st.status;
-    S.stats->iterations = st.iters;
-    S.stats->restarts = st.restarts;
-    S.stats->refinements = st.updates;
-    S.stats->err_init = st.err_init;
-    S.stats->err_opt = st.status == CUP2D_OK ? st.err_true : st.err_opt;
-    S.stats->norm_ax0 = 0.0;
+  take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
+  if (sp.subtract_mean && !subtract_mean(sm, B, pr.M, pr.x, red, b0, b1)) return false;
+  write_stats(sm, pr.stats, st, st.updates, st.status == CUP2D_OK ? st.err_true : st.err_opt, 0.0);
+  return true;
+}
+
+// first b in [0, nb] with wp[b] >= target (wp strictly increasing)
+__device__ __forceinline__ int64_t cost_lower_bound(const int32_t* __restrict__ wp, int64_t nb, int64_t target) {
+  int64_t lo = 0, hi = nb;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if ((int64_t)__ldg(wp + mid) < target) lo = mid + 1;
+    else hi = mid;
   }
+  return lo;
+}
+
+}  // namespace
+
+// ====================================================== single solves =====
+
+// Three CTAs per SM (80 registers): the passes are bound by per-warp memory
+// latency, and the extra warps outweigh the spills this costs (measured on
+// the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(SolveArgs64 S) {
+  __shared__ Smem sm;
+  const int64_t nb = S.M.nb;
+  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
+  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
+  if (threadIdx.x == 0) {
+    sm.team_rank = blockIdx.x;
+    sm.team_size = gridDim.x;
+  }
+  Pinv<double> pin;
+  pin.load(sm.P, S.P, nullptr);
+  __syncthreads();
+  const Problem64 pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.stats};
+  const SolveParams sp{S.tol_abs, S.tol_rel, 0.0, S.max_restarts, S.max_iter, S.subtract_mean, 0};
+  solve_fp64(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
+}
+
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
+  __shared__ Smem sm;
+  const int64_t nb = S.M.nb;
+  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
+  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
+  if (threadIdx.x == 0) {
+    sm.team_rank = blockIdx.x;
+    sm.team_size = gridDim.x;
+  }
+  Pinv<float> pin;
+  pin.load(sm.P, nullptr, S.P32);
+  __syncthreads();
+  const ProblemMixed pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.stats};
+  const SolveParams sp{S.tol_abs, S.tol_rel, S.reliable_delta, S.max_restarts, S.max_iter, S.subtract_mean,
+                       S.reliable_restart};
+  solve_mixed(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
+}
+
+// ========================================================= batches ========
+//
+// Many independent problems in one cooperative launch.  The grid is split
+// into groups of `team` consecutive CTAs; each group takes problems from a
+// shared queue (largest first, so the tail is short) and solves each one
+// with the same code as a single solve, synchronising on its own bounded
+// barrier.  All groups share the abort flag: a timeout anywhere ends the
+// launch.
+
+template <bool MIXED>
+__device__ __forceinline__ void batch_body(const BatchArgs& A) {
+  __shared__ Smem sm;
+  const int team = A.team;
+  const int g = blockIdx.x / team, rank = blockIdx.x % team;
+  GridBarrier B{A.bars + g, A.abort_flag, (unsigned)team, globaltimer_ns() + A.timeout_ns, 0u, nullptr, 0ull};
+  if (threadIdx.x == 0) {
+    sm.team_rank = rank;
+    sm.team_size = team;
+  }
+  typename std::conditional<MIXED, Pinv<float>, Pinv<double>>::type pin;
+  pin.load(sm.P, A.P, A.P32);
+  __syncthreads();
+  double* red = A.red + (size_t)g * kRedQ * team;
+  while (true) {
+    if (rank == 0 && threadIdx.x == 0) A.slots[g] = atomicAdd(A.queue, 1);
+    if (!B.sync(&sm.flag)) return;
+    if (threadIdx.x == 0) {
+      const int q = __ldcg(A.slots + g);
+      sm.slot = q;
+      if (q < A.nprob) {
+        const int p = __ldg(A.order + q);
+        const MeshView& M = MIXED ? A.pmx[p].M : A.p64[p].M;
+        const int64_t W = __ldg(M.wprefix + M.nb);
+        sm.bounds[0] = cost_lower_bound(M.wprefix, M.nb, W * rank / team);
+        sm.bounds[1] = rank == team - 1 ? M.nb : cost_lower_bound(M.wprefix, M.nb, W * (rank + 1) / team);
+      }
+    }
+    __syncthreads();
+    const int q = sm.slot;
+    if (q >= A.nprob) return;
+    const int p = __ldg(A.order + q);
+    const int64_t sb0 = sm.bounds[0], sb1 = sm.bounds[1];
+    bool ok;
+    if constexpr (MIXED) {
+      const ProblemMixed pr = A.pmx[p];
+      const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
+      ok = solve_mixed(sm, B, pin, pr, A.sp, red, b0, b1, sb0, sb1);
+    } else {
+      const Problem64 pr = A.p64[p];
+      const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
+      ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, sb0, sb1);
+    }
+    if (!ok) return;
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch64(BatchArgs A) {
+  batch_body<false>(A);
+}
+
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch_mixed(BatchArgs A) {
+  batch_body<true>(A);
 }
 
 // ------------------------------------------------------------ launch -----
@@ -724,6 +832,16 @@ cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s) {
 cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s) {
   void* args[] = {const_cast<SolveArgsMixed*>(&a)};
   return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args, 0, s);
+}
+
+int max_coop_grid_batch(int device, bool mixed) {
+  return coop_grid(mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64, device);
+}
+
+cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s) {
+  void* args[] = {const_cast<BatchArgs*>(&a)};
+  return cudaLaunchCooperativeKernel(mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64,
+                                     dim3(grid), dim3(kSolveThreads), args, 0, s);
 }
 
 // ------------------------------------------------------- single ops -------

@@ -73,6 +73,7 @@ int from_cuda(cudaError_t e) {
 struct cup2d_poisson {
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool owns_stream = true;  // false for the problems of a batch (batch stream)
   cup2d_solve_opts opts{};
   // forest
   int32_t bpdx = 0, bpdy = 0, level_max = 0, px = 0, py = 0;
@@ -408,7 +409,7 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   if (h->hstats) cudaFreeHost(h->hstats);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->stream && h->owns_stream) cudaStreamDestroy(h->stream);
   delete h;
   return CUP2D_OK;
 }
@@ -647,6 +648,239 @@ int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n_out, int64_t* nnz_out,
   if (n_out) *n_out = n;
   if (nnz_out) *nnz_out = nnz;
   return CUP2D_OK;
+}
+
+}  // extern "C"
+
+// ================================================================ batches ==
+//
+// A batch is a set of independent problems solved in one cooperative
+// launch (k_bicgstab_batch64 / k_bicgstab_batch_mixed): groups of `team`
+// CTAs take problems largest first from a device queue.  Each problem keeps
+// its own assembled operator and Krylov vectors (a handle without a stream
+// of its own); the per-problem descriptors are rebuilt on the host for each
+// solve because the right-hand sides and solutions are call arguments.
+
+struct cup2d_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cup2d_solve_opts opts{};
+  std::vector<cup2d_poisson*> probs;
+  std::vector<int32_t> order;  // largest first
+  int team = 8;
+  int grid64 = 0, gridmx = 0;
+  DevBuf<Problem64> d_p64;
+  DevBuf<ProblemMixed> d_pmx;
+  DevBuf<int32_t> d_order;
+  DevBuf<double> red;
+  DevBuf<unsigned> bars;
+  DevBuf<int> slots, queue, abort_flag;
+  DevBuf<DevStats> dstats;
+  DevBuf<double> P;  // one P^-1 for all problems (it depends on nothing)
+  DevBuf<float> P32;
+  std::vector<Problem64> h_p64;
+  std::vector<ProblemMixed> h_pmx;
+  std::vector<DevStats> hstats;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+extern "C" {
+
+int cup2d_batch_destroy(cup2d_batch* B) {
+  if (!B) return CUP2D_OK;
+  if (B->stream) cudaStreamSynchronize(B->stream);
+  for (auto* h : B->probs) cup2d_poisson_destroy(h);
+  B->d_p64.release();
+  B->d_pmx.release();
+  B->d_order.release();
+  B->red.release();
+  B->bars.release();
+  B->slots.release();
+  B->queue.release();
+  B->abort_flag.release();
+  B->dstats.release();
+  B->P.release();
+  B->P32.release();
+  if (B->ev0) cudaEventDestroy(B->ev0);
+  if (B->ev1) cudaEventDestroy(B->ev1);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve_opts* opts, cup2d_batch** out) {
+  if (!out || n <= 0 || !forests) return CUP2D_INVALID_ARGUMENT;
+  *out = nullptr;
+  cup2d_solve_opts o;
+  cup2d_default_opts(&o);
+  if (opts) o = *opts;
+  int st = validate_opts(o);
+  if (st) return st;
+  for (int32_t i = 0; i < n; ++i)
+    if ((st = check_forest(&forests[i]))) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CUP2D_NO_DEVICE;
+  }
+  auto* B = new (std::nothrow) cup2d_batch();
+  if (!B) return CUP2D_OOM;
+  B->opts = o;
+  cudaGetDevice(&B->device);
+  if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess) {
+    cup2d_batch_destroy(B);
+    return CUP2D_CUDA_ERROR;
+  }
+  B->grid64 = max_coop_grid_batch(B->device, false);
+  B->gridmx = max_coop_grid_batch(B->device, true);
+  if (B->grid64 <= 0 || B->gridmx <= 0) {
+    cup2d_batch_destroy(B);
+    return CUP2D_CUDA_ERROR;
+  }
+  B->probs.reserve(n);
+  for (int32_t i = 0; i < n; ++i) {
+    auto* h = new (std::nothrow) cup2d_poisson();
+    if (!h) {
+      cup2d_batch_destroy(B);
+      return CUP2D_OOM;
+    }
+    h->device = B->device;
+    h->stream = B->stream;
+    h->owns_stream = false;
+    h->opts = o;
+    B->probs.push_back(h);
+    if ((st = do_assemble(h, &forests[i]))) {
+      cup2d_batch_destroy(B);
+      return st;
+    }
+  }
+  B->order.resize(n);
+  for (int32_t i = 0; i < n; ++i) B->order[i] = i;
+  std::stable_sort(B->order.begin(), B->order.end(),
+                   [&](int32_t a, int32_t b) { return B->probs[a]->nb > B->probs[b]->nb; });
+  const int gmax = std::max(B->grid64, B->gridmx);
+  if ((st = B->d_p64.ensure(n)) || (st = B->d_pmx.ensure(n)) || (st = B->d_order.ensure(n)) ||
+      (st = B->red.ensure((int64_t)kRedQ * gmax)) || (st = B->bars.ensure(gmax)) || (st = B->slots.ensure(gmax)) ||
+      (st = B->queue.ensure(1)) || (st = B->abort_flag.ensure(1)) || (st = B->dstats.ensure(n)) ||
+      (st = B->P.ensure(4096)) || (st = B->P32.ensure(4096))) {
+    cup2d_batch_destroy(B);
+    return st;
+  }
+  if (launch_build_pinv(B->P.p, B->stream) != cudaSuccess ||
+      launch_convert_f64_f32(B->P.p, B->P32.p, 4096, B->stream) != cudaSuccess ||
+      cudaMemcpyAsync(B->d_order.p, B->order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, B->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(B->stream) != cudaSuccess) {
+    cup2d_batch_destroy(B);
+    return CUP2D_CUDA_ERROR;
+  }
+  B->h_p64.resize(n);
+  B->h_pmx.resize(n);
+  B->hstats.resize(n);
+  if (const char* e = std::getenv("CUP2D_BATCH_TEAM")) B->team = std::max(1, std::atoi(e));
+  *out = B;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_set_opts(cup2d_batch* B, const cup2d_solve_opts* opts) {
+  if (!B || !opts) return CUP2D_INVALID_ARGUMENT;
+  int st = validate_opts(*opts);
+  if (st) return st;
+  B->opts = *opts;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_set_team(cup2d_batch* B, int32_t team) {
+  if (!B || team < 1 || team > 256) return CUP2D_INVALID_ARGUMENT;
+  B->team = team;
+  return CUP2D_OK;
+}
+
+int32_t cup2d_batch_size(const cup2d_batch* B) { return B ? (int32_t)B->probs.size() : 0; }
+
+int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i) {
+  if (!B || i < 0 || i >= (int32_t)B->probs.size()) return 0;
+  return B->probs[i]->nb * kBLEN;
+}
+
+int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
+                             cup2d_solve_stats* stats, void* stream) {
+  if (!B || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  const int n = (int)B->probs.size();
+  for (int i = 0; i < n; ++i)
+    if (!d_b[i] || !d_x[i]) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const cup2d_solve_opts& o = B->opts;
+  const bool mixed = o.precision == CUP2D_PREC_MIXED;
+  int st;
+  for (int i = 0; i < n; ++i) {
+    cup2d_poisson* h = B->probs[i];
+    if (mixed && (st = ensure_mixed(h))) return st;
+    const MeshView M = h->mesh.view();
+    if (mixed)
+      B->h_pmx[i] = ProblemMixed{M, d_b[i], d_x[i], h->xo.p, h->f_r.p, h->f_rh.p, h->f_p.p, h->f_nu.p,
+                                 h->f_t.p, h->f_z.p, B->dstats.p + i};
+    else
+      B->h_p64[i] = Problem64{M, d_b[i], d_x[i], h->xo.p, h->r.p, h->rh.p, h->p.p, h->nu.p, h->t.p, h->z.p,
+                              B->dstats.p + i};
+  }
+  const int team = B->team;
+  const int gmax = mixed ? B->gridmx : B->grid64;
+  const int groups = std::max(1, std::min(gmax / team, n));
+  if (groups * team > gmax) return CUP2D_INVALID_ARGUMENT;  // team larger than the device
+  const int grid = groups * team;
+  // per group: barriers of every problem it may take, in 32 bits
+  const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)n * (uint64_t)team;
+  if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
+  if ((mixed ? cudaMemcpyAsync(B->d_pmx.p, B->h_pmx.data(), sizeof(ProblemMixed) * n, cudaMemcpyHostToDevice, s)
+             : cudaMemcpyAsync(B->d_p64.p, B->h_p64.data(), sizeof(Problem64) * n, cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess ||
+      cudaMemsetAsync(B->bars.p, 0, sizeof(unsigned) * groups, s) != cudaSuccess ||
+      cudaMemsetAsync(B->queue.p, 0, sizeof(int), s) != cudaSuccess ||
+      cudaMemsetAsync(B->abort_flag.p, 0, sizeof(int), s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  BatchArgs a{};
+  a.p64 = B->d_p64.p;
+  a.pmx = B->d_pmx.p;
+  a.order = B->d_order.p;
+  a.nprob = n;
+  a.team = team;
+  a.P = B->P.p;
+  a.P32 = B->P32.p;
+  a.red = B->red.p;
+  a.bars = B->bars.p;
+  a.slots = B->slots.p;
+  a.queue = B->queue.p;
+  a.abort_flag = B->abort_flag.p;
+  a.sp = SolveParams{o.tol_abs, o.tol_rel, o.reliable_delta, o.max_restarts, o.max_iter, o.subtract_mean,
+                     o.reliable_restart};
+  a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
+  if (stats) cudaEventRecord(B->ev0, s);
+  const cudaError_t e = launch_bicgstab_batch(a, grid, mixed, s);
+  if (e != cudaSuccess) return from_cuda(e);
+  if (!stats) return CUP2D_OK;
+  cudaEventRecord(B->ev1, s);
+  int aborted = 0;
+  if (cudaMemcpyAsync(B->hstats.data(), B->dstats.p, sizeof(DevStats) * n, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(&aborted, B->abort_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+  for (int i = 0; i < n; ++i) {
+    const DevStats& d = B->hstats[i];
+    stats[i].status = aborted ? CUP2D_TIMEOUT : d.status;
+    stats[i].iterations = d.iterations;
+    stats[i].restarts = d.restarts;
+    stats[i].refinements = d.refinements;
+    stats[i].err_init = d.err_init;
+    stats[i].err_final = d.err_opt;
+    stats[i].rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
+    stats[i].solve_ms = ms;  // the whole batch
+  }
+  return aborted ? CUP2D_TIMEOUT : CUP2D_OK;
 }
 
 }  // extern "C"

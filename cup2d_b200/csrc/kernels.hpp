@@ -131,6 +131,60 @@ struct SolveArgsMixed {
   const int32_t* sbounds;    // [grid+1] SpMV block ranges, balanced by cost
 };
 
+// One problem of a solve: its operator, right-hand side, solution and the
+// Krylov vectors it uses.
+struct Problem64 {
+  MeshView M;
+  const double* b;
+  double* x;
+  double* xo;
+  double* r;
+  double* rh;
+  double* p;
+  double* nu;
+  double* t;
+  double* z;
+  DevStats* stats;
+};
+
+struct ProblemMixed {
+  MeshView M;
+  const double* b;
+  double* x;
+  double* xo;
+  float* r;
+  float* rh;
+  float* p;
+  float* nu;
+  float* t;
+  float* z;
+  DevStats* stats;
+};
+
+struct SolveParams {
+  double tol_abs, tol_rel, reliable_delta;
+  int max_restarts, max_iter, subtract_mean, reliable_restart;
+};
+
+// Many problems in one launch: groups of `team` CTAs take problems from a
+// queue in `order` (largest first).
+struct BatchArgs {
+  const Problem64* p64;     // [nprob] (FP64 batches)
+  const ProblemMixed* pmx;  // [nprob] (mixed batches)
+  const int32_t* order;     // [nprob] queue order
+  int nprob;
+  int team;                 // CTAs per problem; the grid is a multiple of it
+  const double* P;          // FP64 P^-1
+  const float* P32;         // FP32 P^-1
+  double* red;              // [groups][kRedQ][team]
+  unsigned* bars;           // [groups] barrier counters, zeroed
+  int* slots;               // [groups]
+  int* queue;               // queue head, zeroed
+  int* abort_flag;          // zeroed
+  SolveParams sp;
+  unsigned long long timeout_ns;
+};
+
 constexpr int kSolveThreads = 256;
 constexpr int kSolveCtasPerSm = 3;
 
@@ -139,6 +193,8 @@ int max_coop_grid_fp64(int device);
 int max_coop_grid_mixed(int device);
 cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s);
 cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s);
+int max_coop_grid_batch(int device, bool mixed);
+cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s);
 
 // Single operations (tests, residual checks).
 cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s);

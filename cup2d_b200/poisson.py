@@ -194,6 +194,72 @@ class Solver:
         return r.value, z.value
 
 
+class BatchSolver:
+    """Many independent problems in one persistent launch (no counterpart in
+    the reference, which solves one problem per PoissonSolver::solve call;
+    each problem here gets exactly that solve)."""
+
+    def __init__(self, meshes: list[Mesh], opts: Optional[L.SolveOpts] = None, team: Optional[int] = None, **kw):
+        self.meshes = list(meshes)
+        self.opts = opts if opts is not None else make_opts(**kw)
+        n = len(self.meshes)
+        forests = (L.Forest * n)(*[m.forest() for m in self.meshes])
+        self._h = C.c_void_p()
+        L.check(L.lib().cup2d_batch_create(n, forests, C.byref(self.opts), C.byref(self._h)), "cup2d_batch_create")
+        if team is not None:
+            self.set_team(team)
+        self.last_stats: Optional[list[dict]] = None
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().cup2d_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self) -> int:
+        return int(L.lib().cup2d_batch_size(self._h))
+
+    def ncells(self, i: int) -> int:
+        return int(L.lib().cup2d_batch_num_cells(self._h, int(i)))
+
+    def set_opts(self, opts: Optional[L.SolveOpts] = None, **kw) -> None:
+        self.opts = opts if opts is not None else make_opts(**kw)
+        L.check(L.lib().cup2d_batch_set_opts(self._h, C.byref(self.opts)), "cup2d_batch_set_opts")
+
+    def set_team(self, team: int) -> None:
+        L.check(L.lib().cup2d_batch_set_team(self._h, int(team)), "cup2d_batch_set_team")
+
+    def solve_device(self, bs, xs, stream=None, stats: bool = True) -> Optional[list[dict]]:
+        """bs[i], xs[i]: contiguous float64 CUDA tensors of problem i; xs hold
+        the initial guesses and receive the solutions."""
+        n = len(self)
+        if len(bs) != n or len(xs) != n:
+            raise ValueError(f"expected {n} right-hand sides and solutions")
+        for i in range(n):
+            _check_dev(bs[i], self.ncells(i))
+            _check_dev(xs[i], self.ncells(i))
+        pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
+        px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
+        st = (L.SolveStats * n)()
+        L.check(L.lib().cup2d_batch_solve_device(self._h, pb, px, st if stats else None, _stream_handle(stream)),
+                "cup2d_batch_solve_device")
+        if stats:
+            self.last_stats = [s.as_dict() for s in st]
+            return self.last_stats
+        return None
+
+
 def _stream_handle(stream) -> C.c_void_p:
     """cudaStream_t of a torch stream; torch's current stream by default."""
     if stream is None:

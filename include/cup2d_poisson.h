@@ -169,6 +169,30 @@ int cup2d_poisson_profile(cup2d_poisson* h, double* compute_ms, double* wait_ms,
 /* Explicit (coarse/fine) rows only: number of rows and non-zeros. */
 int cup2d_poisson_explicit_info(cup2d_poisson* h, int64_t* rows, int64_t* nnz);
 
+/* ------------------------------------------------------------- batches ---- */
+/* Many independent problems solved in one persistent launch.  No counterpart
+ * in the reference, which solves one problem per PoissonSolver::solve call
+ * (source/Poisson/Base.h:12); each problem of a batch gets exactly that solve
+ * (same operator, same BiCGSTAB, same mean removal).  The grid is split into
+ * groups of `team` CTAs that take problems largest first from a device
+ * queue, so uneven sizes balance by work, not by count. */
+typedef struct cup2d_batch cup2d_batch;
+/* Assembles the n operators (one per forest) on the device. */
+int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve_opts* opts,
+                       cup2d_batch** out);
+int cup2d_batch_set_opts(cup2d_batch* B, const cup2d_solve_opts* opts);
+/* CTAs per problem (1..256); 8 by default or $CUP2D_BATCH_TEAM. */
+int cup2d_batch_set_team(cup2d_batch* B, int32_t team);
+int32_t cup2d_batch_size(const cup2d_batch* B);
+int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i);
+/* Solves problem i with RHS d_b[i] and initial guess / solution d_x[i]
+ * (device pointers, arrays of n host-side entries).  Asynchronous on
+ * `stream` unless stats != NULL, in which case stats[0..n-1] are filled
+ * after the launch ends (solve_ms is the whole launch for every entry). */
+int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
+                             cup2d_solve_stats* stats, void* stream);
+int cup2d_batch_destroy(cup2d_batch* B);
+
 /* ------------------------------------------------- synthetic problems ---- */
 typedef struct cup2d_mesh cup2d_mesh;
 /* Forest refined to the finest level where a block meets the band
