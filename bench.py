@@ -1,15 +1,20 @@
 """Benchmark: Poisson solves/s and p50/p99 latency on one B200 (or N replicas).
 
-Workload (default "large"): the block-AMR pressure-Poisson problem of
-bpdx=8, bpdy=4, levelMax=7 refined near 3 seeded disks (20,834 blocks,
-1,333,376 cells), divergence-of-random-Fourier-velocity right-hand sides
-(one seed per step), x0 = 0, solved to relative true L-inf residual 1e-6.
-A step is one solve.  The headline `value` is the mixed-precision solver
-(FP32 Krylov vectors, FP64 solution and true residual); the plain FP64
-solver (the reference's algorithm) is timed on the same right-hand sides
-and reported under "plain_fp64".
+Workload "batch" (default): 512 block-AMR pressure-Poisson problems, each a
+forest refined near 1-3 seeded disks with levelMax 3..6 and a size drawn
+log-uniform in 50..6000 blocks (38.3M cells in total), divergence-of-random-
+Fourier-velocity right-hand sides, x0 = 0, each solved to relative true
+L-inf residual 1e-6.  A step is one batched launch solving all of them.  The
+headline `value` is batched mixed precision (FP32 Krylov vectors, FP64
+solution and true residual); beside it the plain FP64 solver (the
+reference's algorithm, one launch per problem) under "plain_fp64" and
+batched FP64 under "batched_fp64".
+
+Workload "large": one 20,834-block (1,333,376-cell) problem of bpdx=8,
+bpdy=4, levelMax=7 refined near 3 seeded disks; a step is one solve.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batch|large|small]
 
 --impl reference times the reference's algorithm on the host CPU: the C++
 restatement of ExpAMRSolver + BiCGSTABSolver::main (CUP2D's own CPU build
@@ -123,21 +128,23 @@ def algorithmic_bytes(n: int, nb: int, R: int, nnz: int, iters: int, updates: in
     iteration (vector streams) plus the explicit coarse/fine rows and the
     per-block neighbour table read by each of its two SpMVs.
 
-    FP64: 25 vector streams x 8 B per cell.  Mixed: FP32 r, rhat, p, nu, t, z
-    and the FP64 solution x read+written in passes C and E = 116 B per cell;
-    each true-residual refresh reads x, b (FP64) and rhat, writes r (FP32).
-    Matrix: 12 B per stored non-zero (FP64) or 8 B (FP32) + 4 B per stored
-    row, and 28 B per block of structure (neighbours, row mask, row base)."""
+    FP64: 23 vector streams x 8 B per cell (A: R r,p,nu W p,z; B: R z,rhat
+    W nu; C: R r,nu W s,z2; D: R z2,s W t; E: R x,z,z2,s,t,rhat W x,r).
+    Mixed: the same streams with FP32 Krylov vectors and the FP64 solution x
+    (read and written in pass E) = 100 B per cell; each true-residual refresh
+    reads x, b (FP64) and rhat, writes r (FP32).  Matrix: 12 B per stored
+    non-zero (FP64) or 8 B (FP32) + 4 B per stored row, and 28 B per block of
+    structure (neighbours, row mask, row base)."""
     meta = 28.0 * nb
     if precision == "fp64":
         mat = 12.0 * nnz + 4.0 * R + meta
-        per_iter = 25 * 8.0 * n + 2 * mat
+        per_iter = 23 * 8.0 * n + 2 * mat
         setup = (8 + 8 + 8 + 8) * n + mat   # r = b - A x0, rhat: R x,b W r,rhat
         final = 16.0 * n                     # mean removal: R x, W x
         return setup + iters * per_iter + final
     mat32 = 8.0 * nnz + 4.0 * R + meta
     mat64 = 12.0 * nnz + 4.0 * R + meta
-    per_iter = 116.0 * n + 2 * mat32
+    per_iter = 100.0 * n + 2 * mat32
     per_update = (8 + 8 + 4 + 4) * n + mat64
     setup = 8.0 * n + (8 + 8 + 4 + 4) * n + mat64   # sum b; true residual, rhat
     final = 16.0 * n
@@ -145,6 +152,7 @@ def algorithmic_bytes(n: int, nb: int, R: int, nnz: int, iters: int, updates: in
 
 
 def run_ours(args, world, rank, local) -> dict | None:
+    """Single-problem workloads (large, small): a step is one solve."""
     import numpy as np
     import torch
 
@@ -270,6 +278,199 @@ def run_ours(args, world, rank, local) -> dict | None:
     return line
 
 
+def _pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(round(q * (len(v) - 1))))]
+
+
+def batch_sample(meshes, count: int = 32):
+    """Indices of `count` problems evenly spaced in size order (the CPU
+    baseline's bounded sample of the batch)."""
+    import numpy as np
+    order = np.argsort([m.nblocks for m in meshes], kind="stable")
+    return [int(order[int(round(q * (len(meshes) - 1)))]) for q in np.linspace(0.0, 1.0, count)]
+
+
+def oracle_cell_iter_seconds(meshes, seeds, idx, iters: int) -> tuple[float, float, int]:
+    """Oracle (C++/OpenMP restatement of the reference solve) time per cell
+    per BiCGSTAB iteration over `iters` iterations of each sampled problem."""
+    import oracle
+    tot, cells = 0.0, 0
+    for i in idx:
+        A = oracle.Matrix(meshes[i])
+        b = meshes[i].rhs_fourier(seeds[i])
+        t0 = time.perf_counter()
+        A.bicgstab(b, tol_rel=0.0, max_iter=iters, max_restarts=100)
+        tot += time.perf_counter() - t0
+        cells += meshes[i].ncells * iters
+    return tot / cells, tot, oracle.num_threads()
+
+
+def run_batch(args, world, rank, local) -> dict | None:
+    """Batched workload: `--batch` uneven problems (sizes log-uniform in
+    50..6000 blocks), each step one batched solve of all of them from x0 = 0.
+    Headline: batched mixed precision.  Beside it: the plain FP64 solver one
+    problem per launch (the reference's algorithm, the 3x target's base) and
+    batched FP64."""
+    import numpy as np
+    import torch
+
+    from cup2d_b200 import BatchSolver, Solver
+    from cup2d_b200.problems import batch_problems
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    meshes = batch_problems(args.batch, seed=3 + 1000 * rank)
+    n = len(meshes)
+    seeds = [1000 * rank + 100 + i for i in range(n)]
+    hb = [torch.from_numpy(m.rhs_fourier(s)).pin_memory() for m, s in zip(meshes, seeds)]
+    bs = [b.to(dev) for b in hb]
+    xs = [torch.zeros_like(b) for b in bs]
+    cells = [m.ncells for m in meshes]
+    opts = dict(tol_rel=TOL, max_iter=20000, max_restarts=100, timeout_ms=120000)
+    B = BatchSolver(meshes, precision="mixed", team=args.team_mixed, **opts)
+
+    def zero_x():
+        for x in xs:
+            x.zero_()
+
+    def timed_batch(precision: str, team: int):
+        """CUDA events around each batched launch on the launching stream
+        (x0 = 0 written before it); the working set is far above L2."""
+        B.set_opts(precision=precision, **opts)
+        B.set_team(team)
+        ms = []
+        for i in range(args.warmup + args.steps):
+            zero_x()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            B.solve_device(bs, xs, stream=stream, stats=False)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if i >= args.warmup:
+                ms.append(e0.elapsed_time(e1))
+        zero_x()
+        st = B.solve_device(bs, xs, stream=stream)
+        begin, end, _ = B.timeline()
+        return ms, st, end - begin
+
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        ms_mx, st_mx, span_mx = timed_batch("mixed", args.team_mixed)
+    ms_b64, st_b64, _ = timed_batch("fp64", args.team_fp64)
+
+    # plain FP64: one handle per problem, one persistent launch per solve
+    hs = [Solver(m, precision="fp64", **opts) for m in meshes]
+    ms_plain = []
+    for i in range(args.warmup + min(args.steps, args.plain_steps)):
+        zero_x()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for h, b, x in zip(hs, bs, xs):
+            h.solve_device(b, x, stream=stream, stats=False)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            ms_plain.append(e0.elapsed_time(e1))
+    R_nnz = [h.explicit_info() for h in hs]
+    # plain FP64 per-solve latency (one solve at a time, CUDA events)
+    lat_plain = []
+    for h, b, x in zip(hs, bs, xs):
+        x.zero_()
+        lat_plain.append(h.solve_device(b, x, stream=stream)["solve_ms"])
+    for h in hs:
+        h.close()
+
+    # end to end through the public host-buffer API (pinned host memory)
+    B.set_opts(precision="mixed", **opts)
+    B.set_team(args.team_mixed)
+    hx = [torch.zeros(c, dtype=torch.float64).pin_memory() for c in cells]
+    hbn = [b.numpy() for b in hb]
+    hxn = [x.numpy() for x in hx]
+    _barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for x in hxn:
+            x[...] = 0.0
+        B.solve(hbn, hxn)
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    B.close()
+
+    K = args.steps
+    tot_mx = _max_over_ranks(sum(ms_mx), world)
+    tot_b64 = _max_over_ranks(sum(ms_b64), world)
+    tot_plain = _max_over_ranks(sum(ms_plain), world)
+    if rank != 0:
+        return None
+    peak, peak_kind = _peaks()
+    by_mx = sum(algorithmic_bytes(m.ncells, m.nblocks, R, nnz, s["iterations"], s["refinements"], "mixed")
+                for m, (R, nnz), s in zip(meshes, R_nnz, st_mx))
+    by_64 = sum(algorithmic_bytes(m.ncells, m.nblocks, R, nnz, s["iterations"], 0, "fp64")
+                for m, (R, nnz), s in zip(meshes, R_nnz, st_b64))
+    ach_mx = by_mx / (statistics.mean(ms_mx) * 1e-3) / 1e9
+    ach_64 = by_64 / (statistics.mean(ms_b64) * 1e-3) / 1e9
+    cit_mx = sum(s["iterations"] * c for s, c in zip(st_mx, cells))
+    cit_64 = sum(s["iterations"] * c for s, c in zip(st_b64, cells))
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        tj = json.loads(tp.read_text()).get("batch", {})
+        if "dram_bytes_per_cell_iteration_mixed" in tj:
+            traffic = tj["dram_bytes_per_cell_iteration_mixed"] * cit_mx
+    plain_per_s = world * n * len(ms_plain) / (tot_plain * 1e-3)
+    value = world * n * K / (tot_mx * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": tot_mx / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (seeded Fourier-velocity divergence RHS on disk-refined AMR forests)",
+        "config": {"workload": f"batch: {n} problems, sizes log-uniform 50..6000 blocks "
+                               f"({min(m.nblocks for m in meshes)}..{max(m.nblocks for m in meshes)}), "
+                               f"levelMax 3..6, 1-3 disks, {sum(cells)} cells in total, mesh seed {3 + 1000 * rank}",
+                   "tol": "true |b-Ax|_inf / |b|_inf <= 1e-6, x0 = 0 (every problem)",
+                   "solver": f"batched mixed (FP32 Krylov, FP64 x), team {args.team_mixed} CTAs per problem",
+                   "step": f"one launch solving all {n} problems",
+                   "l2": "inputs larger than L2 (working set ~4 GB)", "parallelism": f"replicas x{world}"},
+        "latency_ms": {"step_p50": _pct(ms_mx, 0.5), "step_p99": _pct(ms_mx, 0.99),
+                       "problem_span_p50": float(np.percentile(span_mx, 50)),
+                       "problem_span_p99": float(np.percentile(span_mx, 99))},
+        "iterations_mean": statistics.mean(s["iterations"] for s in st_mx),
+        "true_res_updates_mean": statistics.mean(s["refinements"] for s in st_mx),
+        "plain_fp64": {"value": plain_per_s, "unit": UNIT, "ms_per_step": tot_plain / len(ms_plain),
+                       "how": "one handle and one persistent launch per problem, problems back to back",
+                       "latency_ms": {"p50": _pct(lat_plain, 0.5), "p99": _pct(lat_plain, 0.99)},
+                       "iterations_mean": None},
+        "batched_fp64": {"value": world * n * K / (tot_b64 * 1e-3), "unit": UNIT, "ms_per_step": tot_b64 / K,
+                         "team": args.team_fp64,
+                         "iterations_mean": statistics.mean(s["iterations"] for s in st_b64),
+                         "roofline": {"bound": "hbm", "achieved": ach_64, "peak": peak, "unit": "GB/s",
+                                      "frac": ach_64 / peak, "kernel": "k_bicgstab_batch64"}},
+        "speedup_batched_mixed_vs_plain_fp64": value / plain_per_s,
+        "cell_iterations_per_step": {"mixed": cit_mx, "fp64": cit_64},
+        "roofline": {"bound": "hbm", "achieved": ach_mx, "peak": peak, "unit": "GB/s", "frac": ach_mx / peak,
+                     "traffic": traffic, "kernel": "k_bicgstab_batch_mixed (one launch per step)",
+                     "peak_kind": peak_kind},
+        "e2e": {"value": world * n * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * sum(cells),
+                "d2h_bytes_per_step": 8 * sum(cells)},
+        "gpu_launches": K,
+        "clocks": clk.summary(),
+        "status_ok": all(s["status"] == 0 for s in st_mx + st_b64),
+    }
+    if not args.no_cpu:
+        idx = batch_sample(meshes)
+        sec, tot, cores = oracle_cell_iter_seconds(meshes, seeds, idx, args.cpu_iters)
+        per_solve = sec * cit_64 / n
+        line["cpu_baseline"] = {
+            "value": 1.0 / per_solve, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{args.cpu_iters} BiCGSTAB iterations of each of {len(idx)} problems spread over the size "
+                      f"range ({tot:.1f} s, OpenMP, {cores} threads): {sec * 1e9:.2f} ns per cell-iteration, scaled "
+                      f"by the FP64 cell-iterations of this batch ({cit_64 / n:.3g} per solve)"}
+    return line
+
+
 def cpu_baseline(mesh, b, fp64_iters: float, sample_iters: int = 60) -> dict:
     """The oracle (C++/OpenMP restatement of the reference solve) on the host
     cores: a bounded sample of `sample_iters` BiCGSTAB iterations of the same
@@ -287,9 +488,49 @@ def cpu_baseline(mesh, b, fp64_iters: float, sample_iters: int = 60) -> dict:
                       f"(OpenMP, {cores} threads), scaled by {fp64_iters:.0f} iterations/solve"}
 
 
+def run_reference_batch(args) -> dict:
+    """The reference algorithm on the host cores for the batched workload:
+    the oracle's full solves of a size-quantile sample give iterations per
+    problem (untimed); each step then times a bounded sample of
+    `--cpu-iters` iterations of each sampled problem."""
+    import numpy as np
+
+    import oracle
+    from cup2d_b200.problems import batch_problems
+    meshes = batch_problems(args.batch, seed=3)
+    seeds = [100 + i for i in range(len(meshes))]
+    idx = batch_sample(meshes, args.ref_sample)
+    cores = oracle.num_threads()
+    work = []
+    for i in idx:
+        A = oracle.Matrix(meshes[i])
+        _, st = A.bicgstab(meshes[i].rhs_fourier(seeds[i]), tol_rel=TOL, max_iter=20000, max_restarts=100)
+        work.append(st["iterations"] * meshes[i].ncells)
+    mean_work = float(np.mean(work))  # cell-iterations per solve
+    times = []
+    for k in range(args.warmup + args.steps):
+        sec, _, _ = oracle_cell_iter_seconds(meshes, seeds, idx, args.cpu_iters)
+        if k >= args.warmup:
+            times.append(sec * mean_work)
+    per_solve = statistics.mean(times)
+    v = 1.0 / per_solve
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per_solve * len(meshes) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"batch: {len(meshes)} problems, sizes log-uniform 50..6000 blocks, mesh seed 3",
+                       "tol": "rel 1e-6"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"per step {args.cpu_iters} BiCGSTAB iterations of each of {len(idx)} "
+                                       f"problems spread over the size range (OpenMP, {cores} threads), scaled by "
+                                       f"their full-solve cell-iterations at rel 1e-6 ({mean_work:.3g} per solve)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args, world, rank) -> dict | None:
     if rank != 0:
         return None
+    if args.workload == "batch":
+        return run_reference_batch(args)
     import oracle
     from cup2d_b200.problems import large_mesh, small_mesh
     mesh = large_mesh() if args.workload == "large" else small_mesh()
@@ -328,6 +569,8 @@ def profile_case(args) -> int:
     workload, each capped at `--profile-iters` iterations, one kernel launch
     each.  Prints the solve statistics; no timing is reported."""
     import torch
+    if args.workload == "batch":
+        return profile_batch(args)
 
     from cup2d_b200 import Solver
     from cup2d_b200.problems import large_mesh, small_mesh
@@ -354,13 +597,45 @@ def profile_case(args) -> int:
     return 0
 
 
+def profile_batch(args) -> int:
+    """Two FP64 and two mixed batched launches over the first `--batch`
+    problems of the batched workload, each problem capped at
+    `--profile-iters` iterations."""
+    import torch
+
+    from cup2d_b200 import BatchSolver
+    from cup2d_b200.problems import batch_problems
+    dev = torch.device("cuda", 0)
+    meshes = batch_problems(args.batch, seed=3)
+    bs = [torch.from_numpy(m.rhs_fourier(100 + i)).to(dev) for i, m in enumerate(meshes)]
+    it = args.profile_iters
+    with BatchSolver(meshes, tol_rel=0.0, max_iter=it) as B:
+        for prec, team in (("fp64", args.team_fp64), ("mixed", args.team_mixed)):
+            B.set_opts(tol_rel=0.0, max_iter=it, precision=prec)
+            B.set_team(team)
+            for _ in range(2):
+                xs = [torch.zeros_like(b) for b in bs]
+                st = B.solve_device(bs, xs)
+                _, _, launch_ms = B.timeline()
+                cit = sum(s["iterations"] * m.ncells for s, m in zip(st, meshes))
+                print(f"{prec} team {team}: {launch_ms:.2f} ms, {cit} cell-iterations, "
+                      f"{sum(m.ncells for m in meshes)} cells", flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["large", "small"], default="large")
+    ap.add_argument("--workload", choices=["batch", "large", "small"], default="batch")
+    ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
+    ap.add_argument("--team-mixed", type=int, default=16, help="batch: CTAs per problem, mixed")
+    ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64")
+    ap.add_argument("--plain-steps", type=int, default=3, help="batch: timed steps of the one-at-a-time FP64 leg")
+    ap.add_argument("--cpu-iters", type=int, default=600, help="CPU baseline: iterations per sampled problem")
+    ap.add_argument("--ref-sample", type=int, default=24, help="reference arm: sampled problems")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile-iters", type=int, default=0,
                     help="profiling case: capped solves only (see profile_case)")
@@ -376,7 +651,7 @@ def main(argv=None) -> int:
         line = run_reference(args, world, rank)
     else:
         world, rank, local = _dist()
-        line = run_ours(args, world, rank, local)
+        line = (run_batch if args.workload == "batch" else run_ours)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

@@ -15,22 +15,26 @@
 //
 //   A  p = r + beta (p - omega nu);  z = P^-1 p          (R r,p,nu  W p,z)
 //   B  nu = A z;  (rhat, nu)                             (R z,rhat  W nu)
-//   C  x += alpha z;  s = r - alpha nu;  z = P^-1 s      (R x,z,r,nu W x,r,z)
-//   D  t = A z;  (t,s), (t,t)                            (R z,s     W t)
-//   E  x += omega z;  r = s - omega t;  |r|_inf, (rhat,r), |r|^2, |rhat|^2
-//                                                        (R x,z,s,t,rhat W x,r)
+//   C  s = r - alpha nu;  z2 = P^-1 s                    (R r,nu    W s,z2)
+//   D  t = A z2;  (t,s), (t,t)                           (R z2,s    W t)
+//   E  x += alpha z, x += omega z2;  r = s - omega t;
+//      |r|_inf, (rhat,r), |r|^2, |rhat|^2                (R x,z,z2,s,t,rhat W x,r)
+//
+// The two x updates of the reference (alpha z after the first half step,
+// omega z2 after the second) are applied in that order in pass E, which
+// gives the same values while touching x once per iteration.
 //
 // Scalar recurrences, the breakdown/restart rule (rho^2 < 1e-16|r|^2|rhat|^2),
 // best-iterate tracking and the L-inf stopping test follow the reference.
 // Every CTA reduces the per-CTA partials in the same fixed order (FP64), so
 // all CTAs take identical decisions and results are bitwise reproducible for
-// a given grid.  The best iterate is copied lazily: pass C of the next
+// a given grid.  The best iterate is copied lazily: pass E of the next
 // iteration stores the old x when the previous iterate was the best so far.
 //
 // Mixed form.  A correction accumulated in FP32 loses eps32*kappa of the
 // residual (kappa ~ 1e5..1e7 on these meshes), so restarted FP32 inner
-// solves cannot refine.  Instead x stays FP64 and is updated in passes C and
-// E from the FP32 z; only the Krylov vectors (r, rhat, p, nu, t, z) are
+// solves cannot refine.  Instead x stays FP64 and is updated in pass E from
+// the FP32 z and z2; only the Krylov vectors (r, rhat, p, nu, t, z, z2) are
 // FP32.  When the FP32 residual has dropped by `reliable_delta` since its
 // last replacement, claims convergence, or a sweep stalls, it is replaced by
 // the true residual b - A x computed in FP64 (with b projected to zero sum,
@@ -254,7 +258,8 @@ struct Vecs {
   T* p;
   T* nu;
   T* t;
-  T* z;
+  T* z;   // P^-1 p
+  T* z2;  // P^-1 s
 };
 
 struct IterState {
@@ -285,8 +290,15 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
     float* rh;
     bool set_rh;
     double v[5];
-    __device__ __forceinline__ void operator()(int64_t i, double y) {
-      const double r64 = (__ldg(b + i) - mean_b) - y;
+    struct Pre {
+      double b;
+      float rh;
+    };
+    __device__ __forceinline__ Pre load(int64_t i) const {
+      return Pre{__ldg(b + i), set_rh ? 0.f : __ldcg(rh + i)};
+    }
+    __device__ __forceinline__ void operator()(int64_t i, double y, const Pre& pre) {
+      const double r64 = (pre.b - mean_b) - y;
       const float r32 = (float)r64;
       r[i] = r32;
       float rhv;
@@ -294,7 +306,7 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
         rh[i] = r32;
         rhv = r32;
       } else {
-        rhv = __ldcg(rh + i);
+        rhv = pre.rh;
       }
       v[0] = nanmax(v[0], fabs(r64));
       v[1] += dprod(rhv, r32);
@@ -325,6 +337,8 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
                               int64_t sb0, int64_t sb1, double tol_abs, double tol_rel, int max_restarts,
                               int max_iter, const MixedCtx& mx, IterState& st) {
   constexpr int TB = Pinv<T>::kTile;
+  constexpr int JPW = TB / kWarps;  // blocks of a tile each warp stages
+  static_assert(TB % kWarps == 0, "tile rows per warp");
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const double eps = 1e-21;
   double rho_prev = 1.0, alpha = 1.0, omega = 1.0, beta;
@@ -350,24 +364,44 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       beta = (rho / (rho_prev + eps)) * (alpha / (omega + eps));
     }
     const T tb_beta = (T)beta, tb_omega = (T)omega;
-    // pass A: p = r + beta (p - omega nu); z = P^-1 p
+    // pass A: p = r + beta (p - omega nu); z = P^-1 p.  Each warp loads the
+    // operands of its blocks of the next tile before the tensor-core apply
+    // of the current one, so the loads overlap the apply and its barrier.
     {
+      T rr[JPW][2], pp[JPW][2], nn[JPW][2];
+      auto load = [&](int64_t tb) {
+#pragma unroll
+        for (int jj = 0; jj < JPW; ++jj) {
+          const int64_t blk = tb + w + jj * kWarps;
+          if (blk < b1) {
+            const int64_t o = blk * kBLEN + lane;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              rr[jj][h] = __ldcg(V.r + o + 32 * h);
+              if (!zero_pnu) {
+                pp[jj][h] = __ldcg(V.p + o + 32 * h);
+                nn[jj][h] = __ldcg(V.nu + o + 32 * h);
+              }
+            }
+          }
+        }
+      };
       int buf = 0;
+      if (b0 < b1) load(b0);
       for (int64_t tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
-        for (int j = w; j < TB; j += kWarps) {
+#pragma unroll
+        for (int jj = 0; jj < JPW; ++jj) {
+          const int j = w + jj * kWarps;
           if (j < nvalid) {
-            const int64_t o = (tb + j) * kBLEN;
+            const int64_t o = (tb + j) * kBLEN + lane;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-              const int64_t i = o + lane + 32 * h;
-              const T rv = __ldcg(V.r + i);
-              T pv;
-              if (zero_pnu) pv = rv;
-              else pv = rv + tb_beta * (__ldcg(V.p + i) - tb_omega * __ldcg(V.nu + i));
-              if (restart_now) V.rh[i] = rv;
-              V.p[i] = pv;
+              const T rv = rr[jj][h];
+              const T pv = zero_pnu ? rv : rv + tb_beta * (pp[jj][h] - tb_omega * nn[jj][h]);
+              if (restart_now) V.rh[o + 32 * h] = rv;
+              V.p[o + 32 * h] = pv;
               tile[j][lane + 32 * h] = pv;
             }
           } else {
@@ -375,6 +409,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
             tile[j][lane + 32] = T(0);
           }
         }
+        if (tb + TB < b1) load(tb + TB);
         __syncthreads();
         pin.apply(tile, w, lane, tb, nvalid, V.z);
         buf ^= 1;
@@ -388,9 +423,11 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
         const T* rh;
         T* nu;
         double acc;
-        __device__ __forceinline__ void operator()(int64_t i, T y) {
+        using Pre = T;
+        __device__ __forceinline__ Pre load(int64_t i) const { return __ldcg(rh + i); }
+        __device__ __forceinline__ void operator()(int64_t i, T y, T rhv) {
           nu[i] = y;
-          acc += dprod(__ldcg(rh + i), y);
+          acc += dprod(rhv, y);
         }
       } epi{V.rh, V.nu, 0.0};
       spmv_range<T>(M, V.z, sb0, sb1, epi);
@@ -401,23 +438,37 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     grid_reduce<1>(sm, 0u, red, Q_RHNU);
     alpha = rho / (sm.gres[0] + eps);
     const T ta = (T)alpha;
-    // pass C: x += alpha z; s = r - alpha nu; z = P^-1 s
+    // pass C: s = r - alpha nu (in place of r); z2 = P^-1 s
     {
+      T rr[JPW][2], nn[JPW][2];
+      auto load = [&](int64_t tb) {
+#pragma unroll
+        for (int jj = 0; jj < JPW; ++jj) {
+          const int64_t blk = tb + w + jj * kWarps;
+          if (blk < b1) {
+            const int64_t o = blk * kBLEN + lane;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              rr[jj][h] = __ldcg(V.r + o + 32 * h);
+              nn[jj][h] = __ldcg(V.nu + o + 32 * h);
+            }
+          }
+        }
+      };
       int buf = 0;
+      if (b0 < b1) load(b0);
       for (int64_t tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
-        for (int j = w; j < TB; j += kWarps) {
+#pragma unroll
+        for (int jj = 0; jj < JPW; ++jj) {
+          const int j = w + jj * kWarps;
           if (j < nvalid) {
-            const int64_t o = (tb + j) * kBLEN;
+            const int64_t o = (tb + j) * kBLEN + lane;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-              const int64_t i = o + lane + 32 * h;
-              const X xv = __ldcg(V.x + i);
-              if (st.best_is_x) V.xo[i] = xv;
-              V.x[i] = xv + (X)alpha * (X)__ldcg(V.z + i);
-              const T sv = __ldcg(V.r + i) - ta * __ldcg(V.nu + i);
-              V.r[i] = sv;
+              const T sv = rr[jj][h] - ta * nn[jj][h];
+              V.r[o + 32 * h] = sv;
               tile[j][lane + 32 * h] = sv;
             }
           } else {
@@ -425,25 +476,28 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
             tile[j][lane + 32] = T(0);
           }
         }
+        if (tb + TB < b1) load(tb + TB);
         __syncthreads();
-        pin.apply(tile, w, lane, tb, nvalid, V.z);
+        pin.apply(tile, w, lane, tb, nvalid, V.z2);
         buf ^= 1;
       }
     }
     if (!B.sync(&sm.flag, 3)) return false;
-    // pass D: t = A z; (t,s), (t,t)
+    // pass D: t = A z2; (t,s), (t,t)
     {
       struct Epi {
         const T* s;
         T* t;
         double ts, tt;
-        __device__ __forceinline__ void operator()(int64_t i, T y) {
+        using Pre = T;
+        __device__ __forceinline__ Pre load(int64_t i) const { return __ldcg(s + i); }
+        __device__ __forceinline__ void operator()(int64_t i, T y, T sv) {
           t[i] = y;
-          ts += dprod(y, __ldcg(s + i));
+          ts += dprod(y, sv);
           tt += dprod(y, y);
         }
       } epi{V.r, V.t, 0.0, 0.0};
-      spmv_range<T>(M, V.z, sb0, sb1, epi);
+      spmv_range<T>(M, V.z2, sb0, sb1, epi);
       const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
     }
@@ -451,22 +505,51 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     grid_reduce<2>(sm, 0u, red, Q_TS);
     omega = sm.gres[0] / (sm.gres[1] + eps);
     const T to = (T)omega;
-    // pass E: x += omega z; r = s - omega t; norms
+    // pass E: x += alpha z, then x += omega z2 (the reference's two axpys,
+    // fused into one pass); r = s - omega t; norms.  The best iterate is
+    // saved lazily here: x still holds the previous iterate.  Each warp
+    // issues the loads of two blocks before using either.
     {
       double v[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-        const int64_t o = blk * kBLEN;
+      constexpr int U = 2;
+      for (int64_t base = b0 + w; base < b1; base += U * kWarps) {
+        X xv[U][2];
+        T zv[U][2], z2v[U][2], sv[U][2], tv[U][2], rhv[U][2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int64_t i = o + lane + 32 * h;
-          V.x[i] = __ldcg(V.x + i) + (X)omega * (X)__ldcg(V.z + i);
-          const T rn = __ldcg(V.r + i) - to * __ldcg(V.t + i);
-          V.r[i] = rn;
-          const T rhv = __ldcg(V.rh + i);
-          v[0] = nanmax(v[0], fabs((double)rn));
-          v[1] += dprod(rhv, rn);
-          v[2] += dprod(rn, rn);
-          v[3] += dprod(rhv, rhv);
+        for (int u = 0; u < U; ++u) {
+          const int64_t blk = base + u * kWarps;
+          if (blk < b1) {
+            const int64_t o = blk * kBLEN + lane;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              xv[u][h] = __ldcg(V.x + o + 32 * h);
+              zv[u][h] = __ldcg(V.z + o + 32 * h);
+              z2v[u][h] = __ldcg(V.z2 + o + 32 * h);
+              sv[u][h] = __ldcg(V.r + o + 32 * h);
+              tv[u][h] = __ldcg(V.t + o + 32 * h);
+              rhv[u][h] = __ldcg(V.rh + o + 32 * h);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t blk = base + u * kWarps;
+          if (blk < b1) {
+            const int64_t o = blk * kBLEN + lane;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int64_t i = o + 32 * h;
+              if (st.best_is_x) V.xo[i] = xv[u][h];
+              const X x1 = xv[u][h] + (X)alpha * (X)zv[u][h];
+              V.x[i] = x1 + (X)omega * (X)z2v[u][h];
+              const T rn = sv[u][h] - to * tv[u][h];
+              V.r[i] = rn;
+              v[0] = nanmax(v[0], fabs((double)rn));
+              v[1] += dprod(rhv[u][h], rn);
+              v[2] += dprod(rn, rn);
+              v[3] += dprod(rhv[u][h], rhv[u][h]);
+            }
+          }
         }
       }
       cta_partials<4>(sm, v, 0x1u, red, Q_RMAX);
@@ -596,7 +679,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
                            const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
                            int64_t sb1) {
   const MeshView& M = pr.M;
-  const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z};
+  const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
   {
     struct Epi {
@@ -604,8 +687,10 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
       double* r;
       double* rh;
       double v[3];
-      __device__ __forceinline__ void operator()(int64_t i, double y) {
-        const double rv = __ldg(b + i) - y;
+      using Pre = double;
+      __device__ __forceinline__ Pre load(int64_t i) const { return __ldg(b + i); }
+      __device__ __forceinline__ void operator()(int64_t i, double y, double bi) {
+        const double rv = bi - y;
         r[i] = rv;
         rh[i] = rv;
         v[0] = nanmax(v[0], fabs(y));
@@ -644,7 +729,7 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
                             const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
                             int64_t sb1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z};
+  const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // Neumann compatibility: project b to zero sum (sum b / n)
   {
     double v[1] = {0.0};
@@ -722,7 +807,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
   Pinv<double> pin;
   pin.load(sm.P, S.P, nullptr);
   __syncthreads();
-  const Problem64 pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.stats};
+  const Problem64 pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
   const SolveParams sp{S.tol_abs, S.tol_rel, 0.0, S.max_restarts, S.max_iter, S.subtract_mean, 0};
   solve_fp64(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
 }
@@ -740,7 +825,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   Pinv<float> pin;
   pin.load(sm.P, nullptr, S.P32);
   __syncthreads();
-  const ProblemMixed pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.stats};
+  const ProblemMixed pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
   const SolveParams sp{S.tol_abs, S.tol_rel, S.reliable_delta, S.max_restarts, S.max_iter, S.subtract_mean,
                        S.reliable_restart};
   solve_mixed(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
@@ -772,7 +857,9 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
   while (true) {
     if (rank == 0 && threadIdx.x == 0) A.slots[g] = atomicAdd(A.queue, 1);
     if (!B.sync(&sm.flag)) return;
+    unsigned long long t_begin = 0;
     if (threadIdx.x == 0) {
+      t_begin = globaltimer_ns();
       const int q = __ldcg(A.slots + g);
       sm.slot = q;
       if (q < A.nprob) {
@@ -799,6 +886,11 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
       ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, sb0, sb1);
     }
     if (!ok) return;
+    if (rank == 0 && threadIdx.x == 0) {
+      DevStats* ds = MIXED ? A.pmx[p].stats : A.p64[p].stats;
+      ds->t_begin = t_begin;
+      ds->t_end = globaltimer_ns();
+    }
   }
 }
 

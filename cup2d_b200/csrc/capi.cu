@@ -87,9 +87,9 @@ struct cup2d_poisson {
   DevBuf<int> err;
   DeviceMesh mesh;
   // Krylov vectors (FP64)
-  DevBuf<double> xo, r, rh, p, nu, t, z, bstage, xstage;
+  DevBuf<double> xo, r, rh, p, nu, t, z, z2, bstage, xstage;
   // mixed-precision vectors
-  DevBuf<float> f_r, f_rh, f_p, f_nu, f_t, f_z;
+  DevBuf<float> f_r, f_rh, f_p, f_nu, f_t, f_z, f_z2;
   // persistent-kernel scratch
   DevBuf<double> red;
   DevBuf<unsigned> bar;
@@ -170,7 +170,8 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
     return st;
   // Krylov vectors
   if ((st = h->xo.ensure(n)) || (st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) ||
-      (st = h->nu.ensure(n)) || (st = h->t.ensure(n)) || (st = h->z.ensure(n)))
+      (st = h->nu.ensure(n)) || (st = h->t.ensure(n)) || (st = h->z.ensure(n)) ||
+      (st = h->z2.ensure(n)))
     return st;
   cudaStream_t s = h->stream;
   if (cudaMemcpyAsync(h->level.p, f->level, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -253,7 +254,8 @@ int ensure_mixed(cup2d_poisson* h) {
   const int64_t n = h->nb * kBLEN;
   int st;
   if ((st = h->f_r.ensure(n)) || (st = h->f_rh.ensure(n)) || (st = h->f_p.ensure(n)) ||
-      (st = h->f_nu.ensure(n)) || (st = h->f_t.ensure(n)) || (st = h->f_z.ensure(n)))
+      (st = h->f_nu.ensure(n)) || (st = h->f_t.ensure(n)) || (st = h->f_z.ensure(n)) ||
+      (st = h->f_z2.ensure(n)))
     return st;
   return CUP2D_OK;
 }
@@ -395,10 +397,10 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   for (auto* b : i32) b->release();
   h->xmask.release();
   DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
-                           &h->z, &h->bstage, &h->xstage, &h->red};
+                           &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
   for (auto* b : f64) b->release();
   DevBuf<float>* f32[] = {&h->xval32, &h->P32, &h->f_r, &h->f_rh, &h->f_p,
-                          &h->f_nu, &h->f_t, &h->f_z};
+                          &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
   for (auto* b : f32) b->release();
   h->err.release();
   h->bar.release();
@@ -457,6 +459,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.nu = h->f_nu.p;
     a.t = h->f_t.p;
     a.z = h->f_z.p;
+    a.z2 = h->f_z2.p;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
@@ -485,6 +488,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.nu = h->nu.p;
     a.t = h->t.p;
     a.z = h->z.p;
+    a.z2 = h->z2.p;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
@@ -681,7 +685,11 @@ struct cup2d_batch {
   std::vector<Problem64> h_p64;
   std::vector<ProblemMixed> h_pmx;
   std::vector<DevStats> hstats;
+  std::vector<const double*> stage_b;  // host-buffer solves: per-problem device copies
+  std::vector<double*> stage_x;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  bool have_timeline = false;
 };
 
 extern "C" {
@@ -778,6 +786,8 @@ int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve
   B->h_p64.resize(n);
   B->h_pmx.resize(n);
   B->hstats.resize(n);
+  B->stage_b.resize(n);
+  B->stage_x.resize(n);
   if (const char* e = std::getenv("CUP2D_BATCH_TEAM")) B->team = std::max(1, std::atoi(e));
   *out = B;
   return CUP2D_OK;
@@ -820,9 +830,9 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
     const MeshView M = h->mesh.view();
     if (mixed)
       B->h_pmx[i] = ProblemMixed{M, d_b[i], d_x[i], h->xo.p, h->f_r.p, h->f_rh.p, h->f_p.p, h->f_nu.p,
-                                 h->f_t.p, h->f_z.p, B->dstats.p + i};
+                                 h->f_t.p, h->f_z.p, h->f_z2.p, B->dstats.p + i};
     else
-      B->h_p64[i] = Problem64{M, d_b[i], d_x[i], h->xo.p, h->r.p, h->rh.p, h->p.p, h->nu.p, h->t.p, h->z.p,
+      B->h_p64[i] = Problem64{M, d_b[i], d_x[i], h->xo.p, h->r.p, h->rh.p, h->p.p, h->nu.p, h->t.p, h->z.p, h->z2.p,
                               B->dstats.p + i};
   }
   const int team = B->team;
@@ -869,6 +879,8 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
     return CUP2D_CUDA_ERROR;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+  B->last_ms = ms;
+  B->have_timeline = !aborted;
   for (int i = 0; i < n; ++i) {
     const DevStats& d = B->hstats[i];
     stats[i].status = aborted ? CUP2D_TIMEOUT : d.status;
@@ -878,9 +890,52 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
     stats[i].err_init = d.err_init;
     stats[i].err_final = d.err_opt;
     stats[i].rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
-    stats[i].solve_ms = ms;  // the whole batch
+    stats[i].solve_ms = aborted ? ms : (double)(d.t_end - d.t_begin) * 1e-6;  // this problem's own span
   }
   return aborted ? CUP2D_TIMEOUT : CUP2D_OK;
+}
+
+int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x, cup2d_solve_stats* stats) {
+  if (!B || !b || !x) return CUP2D_INVALID_ARGUMENT;
+  const int n = (int)B->probs.size();
+  cudaStream_t s = B->stream;
+  int st;
+  for (int i = 0; i < n; ++i) {
+    if (!b[i] || !x[i]) return CUP2D_INVALID_ARGUMENT;
+    cup2d_poisson* h = B->probs[i];
+    const int64_t m = h->nb * kBLEN;
+    if ((st = h->bstage.ensure(m)) || (st = h->xstage.ensure(m))) return st;
+    B->stage_b[i] = h->bstage.p;
+    B->stage_x[i] = h->xstage.p;
+    if (cudaMemcpyAsync(h->bstage.p, b[i], sizeof(double) * m, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(h->xstage.p, x[i], sizeof(double) * m, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return CUP2D_CUDA_ERROR;
+  }
+  std::vector<cup2d_solve_stats> local;
+  if (!stats) {
+    local.resize(n);
+    stats = local.data();
+  }
+  st = cup2d_batch_solve_device(B, B->stage_b.data(), B->stage_x.data(), stats, s);
+  if (st != CUP2D_OK) return st;
+  for (int i = 0; i < n; ++i)
+    if (cudaMemcpyAsync(x[i], B->stage_x[i], sizeof(double) * B->probs[i]->nb * kBLEN, cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess)
+      return CUP2D_CUDA_ERROR;
+  return cudaStreamSynchronize(s) == cudaSuccess ? CUP2D_OK : CUP2D_CUDA_ERROR;
+}
+
+int cup2d_batch_timeline(const cup2d_batch* B, double* begin_ms, double* end_ms, double* launch_ms) {
+  if (!B || !begin_ms || !end_ms || !B->have_timeline) return CUP2D_INVALID_ARGUMENT;
+  const int n = (int)B->probs.size();
+  unsigned long long t0 = ~0ull;
+  for (int i = 0; i < n; ++i) t0 = std::min(t0, B->hstats[i].t_begin);
+  for (int i = 0; i < n; ++i) {
+    begin_ms[i] = (double)(B->hstats[i].t_begin - t0) * 1e-6;
+    end_ms[i] = (double)(B->hstats[i].t_end - t0) * 1e-6;
+  }
+  if (launch_ms) *launch_ms = B->last_ms;
+  return CUP2D_OK;
 }
 
 }  // extern "C"

@@ -95,7 +95,13 @@ struct GridBarrier {
       red_release_add_u32(counter, 1u);
       const unsigned target = epoch * nparties;
       unsigned spins = 0;
-      while (ld_acquire_u32(counter) < target) {
+      // the deadline bounds the whole launch: checked at every barrier (a
+      // register read), the abort flag only while spinning
+      if (globaltimer_ns() > deadline_ns) {
+        atomicExch(abort_flag, 1);
+        ok = 0;
+      }
+      while (ok && ld_acquire_u32(counter) < target) {
         if ((++spins & 63u) == 0) {
           if (ld_volatile_s32(abort_flag) != 0 || globaltimer_ns() > deadline_ns) {
             atomicExch(abort_flag, 1);

@@ -79,7 +79,7 @@ struct DevStats {
   double err_init;
   double err_opt;
   double norm_ax0;
-  double pad;
+  unsigned long long t_begin, t_end;  // batch: globaltimer ns when the team took / finished the problem
 };
 
 constexpr int kRedQ = 20;  // reduction quantities per CTA
@@ -95,7 +95,8 @@ struct SolveArgs64 {
   double* p;
   double* nu;
   double* t;
-  double* z;
+  double* z;            // P^-1 p
+  double* z2;           // P^-1 s
   double* red;          // [kRedQ][grid]
   unsigned* bar;        // arrival counter, zeroed before launch
   int* abort_flag;      // zeroed before launch
@@ -119,7 +120,8 @@ struct SolveArgsMixed {
   float* p;
   float* nu;
   float* t;
-  float* z;
+  float* z;             // P^-1 p
+  float* z2;            // P^-1 s
   double* red;
   unsigned* bar;
   int* abort_flag;
@@ -144,6 +146,7 @@ struct Problem64 {
   double* nu;
   double* t;
   double* z;
+  double* z2;
   DevStats* stats;
 };
 
@@ -158,6 +161,7 @@ struct ProblemMixed {
   float* nu;
   float* t;
   float* z;
+  float* z2;
   DevStats* stats;
 };
 
@@ -186,7 +190,10 @@ struct BatchArgs {
 };
 
 constexpr int kSolveThreads = 256;
-constexpr int kSolveCtasPerSm = 3;
+#ifndef CUP2D_CTAS_PER_SM
+#define CUP2D_CTAS_PER_SM 3
+#endif
+constexpr int kSolveCtasPerSm = CUP2D_CTAS_PER_SM;
 
 // Largest co-resident grid of the persistent kernels on this device.
 int max_coop_grid_fp64(int device);

@@ -15,7 +15,7 @@
 // Limits and rules (also in include/cup2d_poisson.h):
 //  * at most kNoAllocMaxBlocks = 4096 blocks (262,144 cells) and 1024 CTAs;
 //    larger problems are rejected with CUP2D_INVALID_ARGUMENT;
-//  * the array is 14.2 MiB of static device memory that every GPU which
+//  * the array is 16.2 MiB of static device memory that every GPU which
 //    loads the library holds until the process exits;
 //  * all calls share the array, which keeps the last call's contents; calls
 //    whose work overlaps on the GPU (other streams, other threads) race, so
@@ -46,8 +46,8 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Scratch layout (byte offsets, 256-byte aligned)
 constexpr size_t kVecBytes = align256(sizeof(double) * kNoAllocMaxCells);
-constexpr size_t kOffVec = 0;  // xo, r, rh, p, nu, t, z
-constexpr size_t kOffRed = kOffVec + 7 * kVecBytes;
+constexpr size_t kOffVec = 0;  // xo, r, rh, p, nu, t, z, z2
+constexpr size_t kOffRed = kOffVec + 8 * kVecBytes;
 constexpr size_t kOffBounds = kOffRed + align256(sizeof(double) * kRedQ * kNoAllocMaxGrid);
 constexpr size_t kOffBar = kOffBounds + align256(sizeof(int32_t) * (kNoAllocMaxGrid + 1));
 constexpr size_t kOffAbort = kOffBar + 256;
@@ -132,6 +132,7 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   a.nu = vec + 4 * stride;
   a.t = vec + 5 * stride;
   a.z = vec + 6 * stride;
+  a.z2 = vec + 7 * stride;
   a.red = reinterpret_cast<double*>(base + kOffRed);
   a.bar = reinterpret_cast<unsigned*>(base + kOffBar);
   a.abort_flag = reinterpret_cast<int*>(base + kOffAbort);

@@ -4,9 +4,9 @@
 // cells c0 = l (rows iy = 0..3) and c1 = l + 32 (rows 4..7).  In-block
 // neighbours come from warp shuffles; cells across a same-level face are
 // read from the neighbour block, and a wall face contributes no flux.
-// Loads of two blocks are issued before either is computed so that each
-// warp keeps two blocks' worth of requests in flight.  Rows of cells on a
-// coarse/fine face are skipped here.
+// Loads of two blocks (and the epilogue's operands) are issued before either
+// is computed so that each warp keeps two blocks' worth of requests in
+// flight.  Rows of cells on a coarse/fine face are skipped here.
 //
 // Phase 2 (explicit rows): every thread of the CTA takes explicit rows of
 // the range (they are numbered contiguously by block), one row each.
@@ -49,10 +49,10 @@ struct BlockGather {
 };
 
 template <class T>
-__device__ __forceinline__ void gather_block(const MeshView& M, int64_t blk, const T* __restrict__ z, int lane,
-                                             BlockGather<T>& g) {
+__device__ __forceinline__ void gather_block_nb(const int4& nb, int64_t blk, const T* __restrict__ z, int lane,
+                                                BlockGather<T>& g) {
   const int ix = lane & 7, iy0 = lane >> 3;
-  g.nb = __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
+  g.nb = nb;
   const int64_t o = blk * kBLEN;
   g.z0 = ldcg(z + o + lane);
   g.z1 = ldcg(z + o + lane + 32);
@@ -69,6 +69,16 @@ __device__ __forceinline__ void gather_block(const MeshView& M, int64_t blk, con
   }
   if (iy0 == 0 && g.nb.z >= 0) g.ym = ldcg(z + (int64_t)g.nb.z * kBLEN + 56 + ix);
   if (iy0 == 3 && g.nb.w >= 0) g.yp = ldcg(z + (int64_t)g.nb.w * kBLEN + ix);
+}
+
+__device__ __forceinline__ int4 block_nbr(const MeshView& M, int64_t blk) {
+  return __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
+}
+
+template <class T>
+__device__ __forceinline__ void gather_block(const MeshView& M, int64_t blk, const T* __restrict__ z, int lane,
+                                             BlockGather<T>& g) {
+  gather_block_nb<T>(block_nbr(M, blk), blk, z, lane, g);
 }
 
 // Stencil rows of the gathered block (explicit rows get meaningless values).
@@ -118,32 +128,55 @@ __device__ __forceinline__ void spmv_block(const MeshView& M, int64_t blk, const
   }
 }
 
-// y = A z over blocks [b0, b1) by the whole CTA; epi(i, y_i) is called once
-// per cell (by the thread that computed it), in no particular order.
+// y = A z over blocks [b0, b1) by the whole CTA.  The epilogue is a functor
+// with `Pre load(i)`, the operands it needs at cell i (loaded together with
+// the gather, before y is known), and `operator()(i, y, pre)`, called once
+// per cell by the thread that computed it, in no particular order.  The
+// neighbour tables of a warp's next block pair are fetched while it
+// computes the current pair, so each pair costs one round trip to memory.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int64_t b0, int64_t b1,
                                            Epi& epi) {
+  using Pre = typename Epi::Pre;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int64_t blk = b0 + w; blk < b1; blk += 2 * nw) {
+  int64_t blk = b0 + w;
+  int4 na = make_int4(0, 0, 0, 0), nbb = make_int4(0, 0, 0, 0);
+  if (blk < b1) na = block_nbr(M, blk);
+  if (blk + nw < b1) nbb = block_nbr(M, blk + nw);
+  for (; blk < b1; blk += 2 * nw) {
     const bool two = blk + nw < b1;  // warp-uniform
     BlockGather<T> ga, gb;
-    gather_block<T>(M, blk, z, lane, ga);
-    if (two) gather_block<T>(M, blk + nw, z, lane, gb);
+    gather_block_nb<T>(na, blk, z, lane, ga);
+    const int64_t oa = blk * kBLEN, ob = (blk + nw) * kBLEN;
+    const Pre pa0 = epi.load(oa + lane), pa1 = epi.load(oa + lane + 32);
+    Pre pb0{}, pb1{};
+    if (two) {
+      gather_block_nb<T>(nbb, blk + nw, z, lane, gb);
+      pb0 = epi.load(ob + lane);
+      pb1 = epi.load(ob + lane + 32);
+    }
+    const int64_t nxt = blk + 2 * nw;
+    if (nxt < b1) na = block_nbr(M, nxt);
+    if (nxt + nw < b1) nbb = block_nbr(M, nxt + nw);
     T y0, y1;
     stencil_block<T>(ga, lane, y0, y1);
     unsigned long long m = explicit_mask<T>(M, blk, ga.nb);
-    if (!((m >> lane) & 1ull)) epi(blk * kBLEN + lane, y0);
-    if (!((m >> (lane + 32)) & 1ull)) epi(blk * kBLEN + lane + 32, y1);
+    if (!((m >> lane) & 1ull)) epi(oa + lane, y0, pa0);
+    if (!((m >> (lane + 32)) & 1ull)) epi(oa + lane + 32, y1, pa1);
     if (two) {
       stencil_block<T>(gb, lane, y0, y1);
       m = explicit_mask<T>(M, blk + nw, gb.nb);
-      if (!((m >> lane) & 1ull)) epi((blk + nw) * kBLEN + lane, y0);
-      if (!((m >> (lane + 32)) & 1ull)) epi((blk + nw) * kBLEN + lane + 32, y1);
+      if (!((m >> lane) & 1ull)) epi(ob + lane, y0, pb0);
+      if (!((m >> (lane + 32)) & 1ull)) epi(ob + lane + 32, y1, pb1);
     }
   }
   if (b1 > b0) {
     const int r0 = __ldg(M.xbase + b0), r1 = __ldg(M.xbase + b1);
-    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) epi((int64_t)__ldg(M.rowcell + r), explicit_row<T>(M, r, z));
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const int64_t i = (int64_t)__ldg(M.rowcell + r);
+      const Pre pre = epi.load(i);
+      epi(i, explicit_row<T>(M, r, z), pre);
+    }
   }
 }
 

@@ -133,7 +133,7 @@ class Solver:
         """The FP64 device solve without any device allocation, for callers
         that must not allocate at solve time (their device memory belongs to
         their own pool, or their loop cannot afford the synchronisation an
-        allocation can cause).  Scratch lives in one static 14.2 MiB device
+        allocation can cause).  Scratch lives in one static 16.2 MiB device
         array shared by all calls: at most CUP2D_NOALLOC_MAX_BLOCKS (4096)
         blocks, and calls that overlap on the GPU race."""
         _check_dev(b, self.ncells)
@@ -258,6 +258,33 @@ class BatchSolver:
             self.last_stats = [s.as_dict() for s in st]
             return self.last_stats
         return None
+
+    def solve(self, bs, xs) -> list[dict]:
+        """Host arrays (contiguous float64, e.g. pinned): xs[i] holds the
+        initial guess and receives the solution; the copies are part of the
+        call."""
+        n = len(self)
+        if len(bs) != n or len(xs) != n:
+            raise ValueError(f"expected {n} right-hand sides and solutions")
+        for i in range(n):
+            for a in (bs[i], xs[i]):
+                if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != self.ncells(i):
+                    raise ValueError(f"problem {i}: expected contiguous float64 arrays of {self.ncells(i)} cells")
+        pb = (L.P_f64 * n)(*[_pd(a) for a in bs])
+        px = (L.P_f64 * n)(*[_pd(a) for a in xs])
+        st = (L.SolveStats * n)()
+        L.check(L.lib().cup2d_batch_solve(self._h, pb, px, st), "cup2d_batch_solve")
+        self.last_stats = [s.as_dict() for s in st]
+        return self.last_stats
+
+    def timeline(self) -> tuple[np.ndarray, np.ndarray, float]:
+        """(begin_ms, end_ms, launch_ms) of the last solve that returned stats."""
+        n = len(self)
+        b = np.empty(n)
+        e = np.empty(n)
+        t = C.c_double()
+        L.check(L.lib().cup2d_batch_timeline(self._h, _pd(b), _pd(e), C.byref(t)), "cup2d_batch_timeline")
+        return b, e, t.value
 
 
 def _stream_handle(stream) -> C.c_void_p:

@@ -65,3 +65,11 @@ def sized_mesh(rng: np.random.Generator, target_blocks: int, level_max: int | No
 
 def loguniform_sizes(rng: np.random.Generator, count: int, lo: int, hi: int) -> np.ndarray:
     return np.exp(rng.uniform(math.log(lo), math.log(hi), size=count)).astype(np.int64)
+
+
+def batch_problems(count: int = 512, seed: int = 3, lo: int = 50, hi: int = 6000) -> list[Mesh]:
+    """The batched workload: `count` disk-refined meshes with sizes drawn
+    log-uniform in [lo, hi] blocks (levelMax 3..6, 1-3 disks each)."""
+    rng = np.random.default_rng(seed)
+    sizes = loguniform_sizes(rng, count, lo, hi)
+    return [sized_mesh(rng, int(s)) for s in sizes]

@@ -76,7 +76,8 @@ typedef struct cup2d_solve_opts {
   double reliable_delta;   /* mixed: once the FP32 residual has dropped by this factor
                               since the last replacement, replace it by the true FP64
                               residual b - A x */
-  int32_t timeout_ms;      /* bound on every device-side wait */
+  int32_t timeout_ms;      /* bound on the device time of a launch, checked at every
+                              barrier; a wait for another CTA also ends there */
   int32_t reliable_restart;/* mixed: 1 restarts the BiCGSTAB recurrences (rhat = r,
                               p = nu = 0) at each replacement: FP64 iterative
                               refinement of restarted FP32 BiCGSTAB sweeps whose
@@ -135,7 +136,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
  * device-wide synchronisation cudaMalloc/cudaFree can cause.  The handle's
  * operator (built at create/update time) and the caller's b and x are the
  * inputs and outputs; every scratch buffer of the solve lives in one static
- * device array of 14.2 MiB that each GPU loading the library holds until
+ * device array of 16.2 MiB that each GPU loading the library holds until
  * exit.  Limits: at most CUP2D_NOALLOC_MAX_BLOCKS blocks (larger problems
  * return CUP2D_INVALID_ARGUMENT) and always the plain FP64 form.  All calls
  * share the array: calls whose GPU work overlaps race, so serialise them.
@@ -188,9 +189,18 @@ int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i);
 /* Solves problem i with RHS d_b[i] and initial guess / solution d_x[i]
  * (device pointers, arrays of n host-side entries).  Asynchronous on
  * `stream` unless stats != NULL, in which case stats[0..n-1] are filled
- * after the launch ends (solve_ms is the whole launch for every entry). */
+ * after the launch ends (solve_ms: the problem's own span inside the
+ * launch, from its team taking it to its solution written). */
 int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
                              cup2d_solve_stats* stats, void* stream);
+/* Same on host buffers (b[i] the RHS, x[i] initial guess in, solution out);
+ * the copies are part of the call, on the batch's own stream. */
+int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x,
+                      cup2d_solve_stats* stats);
+/* Schedule of the last solve that returned stats: when each problem's team
+ * took it and finished it, in ms from the first start, and the launch's
+ * duration (CUDA events); for tuning the team size. */
+int cup2d_batch_timeline(const cup2d_batch* B, double* begin_ms, double* end_ms, double* launch_ms);
 int cup2d_batch_destroy(cup2d_batch* B);
 
 /* ------------------------------------------------- synthetic problems ---- */
