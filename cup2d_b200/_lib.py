@@ -76,6 +76,8 @@ SIGNATURES = {
                                            C.POINTER(SolveStats), C.c_void_p]),
     "cup2d_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(P_f64), C.POINTER(P_f64), C.POINTER(SolveStats)]),
     "cup2d_batch_timeline": (C.c_int, [C.c_void_p, P_f64, P_f64, P_f64]),
+    "cup2d_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cup2d_batch_profile": (C.c_int, [C.c_void_p, P_f64, P_f64, C.c_int32]),
     "cup2d_batch_destroy": (C.c_int, [C.c_void_p]),
     "cup2d_mesh_disks": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                    C.c_int32, P_f64, C.c_double, C.POINTER(C.c_void_p)]),

@@ -277,6 +277,72 @@ struct IterState {
 __device__ __forceinline__ double dprod(double a, double b) { return a * b; }
 __device__ __forceinline__ double dprod(float a, float b) { return (double)a * (double)b; }
 
+// SpMV epilogue of pass B: nu = y, (rhat, nu).
+template <class T>
+struct EpiRhNu {
+  static constexpr int LV = Lane<T>::V;
+  const T* rh;
+  T* nu;
+  double acc;
+  struct Pre {
+    T rh[LV];
+  };
+  __device__ __forceinline__ Pre load(int64_t i0) const {
+    Pre p;
+    ldv<LV>(rh + i0, p.rh);
+    return p;
+  }
+  __device__ __forceinline__ Pre load1(int64_t i) const {
+    Pre p{};
+    p.rh[0] = __ldcg(rh + i);
+    return p;
+  }
+  __device__ __forceinline__ void vec(int64_t i0, const T (&y)[LV], const Pre& p) {
+    stv<LV>(nu + i0, y);
+#pragma unroll
+    for (int j = 0; j < LV; ++j) acc += dprod(p.rh[j], y[j]);
+  }
+  __device__ __forceinline__ void one(int64_t i, T y, const Pre& p, int j) {
+    nu[i] = y;
+    acc += dprod(p.rh[j], y);
+  }
+};
+
+// SpMV epilogue of pass D: t = y, (t, s), (t, t).
+template <class T>
+struct EpiTS {
+  static constexpr int LV = Lane<T>::V;
+  const T* s;
+  T* t;
+  double ts, tt;
+  struct Pre {
+    T s[LV];
+  };
+  __device__ __forceinline__ Pre load(int64_t i0) const {
+    Pre p;
+    ldv<LV>(s + i0, p.s);
+    return p;
+  }
+  __device__ __forceinline__ Pre load1(int64_t i) const {
+    Pre p{};
+    p.s[0] = __ldcg(s + i);
+    return p;
+  }
+  __device__ __forceinline__ void vec(int64_t i0, const T (&y)[LV], const Pre& p) {
+    stv<LV>(t + i0, y);
+#pragma unroll
+    for (int j = 0; j < LV; ++j) {
+      ts += dprod(y[j], p.s[j]);
+      tt += dprod(y[j], y[j]);
+    }
+  }
+  __device__ __forceinline__ void one(int64_t i, T y, const Pre& p, int j) {
+    t[i] = y;
+    ts += dprod(y, p.s[j]);
+    tt += dprod(y, y);
+  }
+};
+
 // Mixed form: r = (b - mean_b) - A x in FP64, stored as FP32 (and as rhat
 // when set_rh); partials |r64|_inf, (rhat,r), |r|^2, |rhat|^2, |r32|_inf.
 __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
@@ -291,28 +357,44 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
     bool set_rh;
     double v[5];
     struct Pre {
-      double b;
-      float rh;
+      double b[2];
+      float rh[2];
     };
-    __device__ __forceinline__ Pre load(int64_t i) const {
-      return Pre{__ldg(b + i), set_rh ? 0.f : __ldcg(rh + i)};
+    __device__ __forceinline__ Pre load(int64_t i0) const {
+      Pre p;
+      ldv<2>(b + i0, p.b);
+      if (set_rh) p.rh[0] = p.rh[1] = 0.f;
+      else ldv<2>(rh + i0, p.rh);
+      return p;
     }
-    __device__ __forceinline__ void operator()(int64_t i, double y, const Pre& pre) {
-      const double r64 = (pre.b - mean_b) - y;
+    __device__ __forceinline__ Pre load1(int64_t i) const {
+      Pre p{};
+      p.b[0] = __ldg(b + i);
+      if (!set_rh) p.rh[0] = __ldcg(rh + i);
+      return p;
+    }
+    __device__ __forceinline__ float acc(double y, double bi, float rhi) {
+      const double r64 = (bi - mean_b) - y;
       const float r32 = (float)r64;
-      r[i] = r32;
-      float rhv;
-      if (set_rh) {
-        rh[i] = r32;
-        rhv = r32;
-      } else {
-        rhv = pre.rh;
-      }
+      const float rhv = set_rh ? r32 : rhi;
       v[0] = nanmax(v[0], fabs(r64));
       v[1] += dprod(rhv, r32);
       v[2] += dprod(r32, r32);
       v[3] += dprod(rhv, rhv);
       v[4] = nanmax(v[4], fabs((double)r32));
+      return r32;
+    }
+    __device__ __forceinline__ void vec(int64_t i0, const double (&y)[2], const Pre& p) {
+      float rr[2];
+      rr[0] = acc(y[0], p.b[0], p.rh[0]);
+      rr[1] = acc(y[1], p.b[1], p.rh[1]);
+      stv<2>(r + i0, rr);
+      if (set_rh) stv<2>(rh + i0, rr);
+    }
+    __device__ __forceinline__ void one(int64_t i, double y, const Pre& p, int j) {
+      const float r32 = acc(y, p.b[j], p.rh[j]);
+      r[i] = r32;
+      if (set_rh) rh[i] = r32;
     }
   } epi{b, mean_b, r, rh, set_rh, {0.0, 0.0, 0.0, 0.0, 0.0}};
   spmv_range<double>(M, x, sb0, sb1, epi);
@@ -337,9 +419,10 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
                               int64_t sb0, int64_t sb1, double tol_abs, double tol_rel, int max_restarts,
                               int max_iter, const MixedCtx& mx, IterState& st) {
   constexpr int TB = Pinv<T>::kTile;
-  constexpr int JPW = TB / kWarps;  // blocks of a tile each warp stages
-  static_assert(TB % kWarps == 0, "tile rows per warp");
+  constexpr int LV = Lane<T>::V, CB = Lane<T>::CB;  // 16-byte lane layout
+  static_assert(TB == CB * kWarps, "one chunk of each tile per warp");
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const Lane<T> L(lane);
   const double eps = 1e-21;
   double rho_prev = 1.0, alpha = 1.0, omega = 1.0, beta;
   bool zero_pnu = true;
@@ -364,25 +447,19 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       beta = (rho / (rho_prev + eps)) * (alpha / (omega + eps));
     }
     const T tb_beta = (T)beta, tb_omega = (T)omega;
-    // pass A: p = r + beta (p - omega nu); z = P^-1 p.  Each warp loads the
-    // operands of its blocks of the next tile before the tensor-core apply
-    // of the current one, so the loads overlap the apply and its barrier.
+    // pass A: p = r + beta (p - omega nu); z = P^-1 p.  Warp w stages chunk w
+    // of each tile and loads its operands of the next tile before the
+    // tensor-core apply of the current one, so the loads overlap the apply.
     {
-      T rr[JPW][2], pp[JPW][2], nn[JPW][2];
+      T rr[LV], pp[LV], nn[LV];
       auto load = [&](int64_t tb) {
-#pragma unroll
-        for (int jj = 0; jj < JPW; ++jj) {
-          const int64_t blk = tb + w + jj * kWarps;
-          if (blk < b1) {
-            const int64_t o = blk * kBLEN + lane;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              rr[jj][h] = __ldcg(V.r + o + 32 * h);
-              if (!zero_pnu) {
-                pp[jj][h] = __ldcg(V.p + o + 32 * h);
-                nn[jj][h] = __ldcg(V.nu + o + 32 * h);
-              }
-            }
+        const int64_t blk = tb + w * CB + L.bl;
+        if (blk < b1) {
+          const int64_t i0 = blk * kBLEN + L.cell0;
+          ldv<LV>(V.r + i0, rr);
+          if (!zero_pnu) {
+            ldv<LV>(V.p + i0, pp);
+            ldv<LV>(V.nu + i0, nn);
           }
         }
       };
@@ -391,24 +468,19 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       for (int64_t tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
+        const int j = w * CB + L.bl;
+        T pv[LV];
+        if (j < nvalid) {
+          const int64_t i0 = (tb + j) * kBLEN + L.cell0;
 #pragma unroll
-        for (int jj = 0; jj < JPW; ++jj) {
-          const int j = w + jj * kWarps;
-          if (j < nvalid) {
-            const int64_t o = (tb + j) * kBLEN + lane;
+          for (int k = 0; k < LV; ++k) pv[k] = zero_pnu ? rr[k] : rr[k] + tb_beta * (pp[k] - tb_omega * nn[k]);
+          if (restart_now) stv<LV>(V.rh + i0, rr);
+          stv<LV>(V.p + i0, pv);
+        } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const T rv = rr[jj][h];
-              const T pv = zero_pnu ? rv : rv + tb_beta * (pp[jj][h] - tb_omega * nn[jj][h]);
-              if (restart_now) V.rh[o + 32 * h] = rv;
-              V.p[o + 32 * h] = pv;
-              tile[j][lane + 32 * h] = pv;
-            }
-          } else {
-            tile[j][lane] = T(0);
-            tile[j][lane + 32] = T(0);
-          }
+          for (int k = 0; k < LV; ++k) pv[k] = T(0);
         }
+        stv<LV>(&tile[j][L.cell0], pv);
         if (tb + TB < b1) load(tb + TB);
         __syncthreads();
         pin.apply(tile, w, lane, tb, nvalid, V.z);
@@ -419,17 +491,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     if (!B.sync(&sm.flag, 1)) return false;
     // pass B: nu = A z; (rhat, nu)
     {
-      struct Epi {
-        const T* rh;
-        T* nu;
-        double acc;
-        using Pre = T;
-        __device__ __forceinline__ Pre load(int64_t i) const { return __ldcg(rh + i); }
-        __device__ __forceinline__ void operator()(int64_t i, T y, T rhv) {
-          nu[i] = y;
-          acc += dprod(rhv, y);
-        }
-      } epi{V.rh, V.nu, 0.0};
+      EpiRhNu<T> epi{V.rh, V.nu, 0.0};
       spmv_range<T>(M, V.z, sb0, sb1, epi);
       const double v[1] = {epi.acc};
       cta_partials<1>(sm, v, 0u, red, Q_RHNU);
@@ -440,19 +502,13 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     const T ta = (T)alpha;
     // pass C: s = r - alpha nu (in place of r); z2 = P^-1 s
     {
-      T rr[JPW][2], nn[JPW][2];
+      T rr[LV], nn[LV];
       auto load = [&](int64_t tb) {
-#pragma unroll
-        for (int jj = 0; jj < JPW; ++jj) {
-          const int64_t blk = tb + w + jj * kWarps;
-          if (blk < b1) {
-            const int64_t o = blk * kBLEN + lane;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              rr[jj][h] = __ldcg(V.r + o + 32 * h);
-              nn[jj][h] = __ldcg(V.nu + o + 32 * h);
-            }
-          }
+        const int64_t blk = tb + w * CB + L.bl;
+        if (blk < b1) {
+          const int64_t i0 = blk * kBLEN + L.cell0;
+          ldv<LV>(V.r + i0, rr);
+          ldv<LV>(V.nu + i0, nn);
         }
       };
       int buf = 0;
@@ -460,22 +516,18 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       for (int64_t tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
+        const int j = w * CB + L.bl;
+        T sv[LV];
+        if (j < nvalid) {
+          const int64_t i0 = (tb + j) * kBLEN + L.cell0;
 #pragma unroll
-        for (int jj = 0; jj < JPW; ++jj) {
-          const int j = w + jj * kWarps;
-          if (j < nvalid) {
-            const int64_t o = (tb + j) * kBLEN + lane;
+          for (int k = 0; k < LV; ++k) sv[k] = rr[k] - ta * nn[k];
+          stv<LV>(V.r + i0, sv);
+        } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const T sv = rr[jj][h] - ta * nn[jj][h];
-              V.r[o + 32 * h] = sv;
-              tile[j][lane + 32 * h] = sv;
-            }
-          } else {
-            tile[j][lane] = T(0);
-            tile[j][lane + 32] = T(0);
-          }
+          for (int k = 0; k < LV; ++k) sv[k] = T(0);
         }
+        stv<LV>(&tile[j][L.cell0], sv);
         if (tb + TB < b1) load(tb + TB);
         __syncthreads();
         pin.apply(tile, w, lane, tb, nvalid, V.z2);
@@ -485,18 +537,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     if (!B.sync(&sm.flag, 3)) return false;
     // pass D: t = A z2; (t,s), (t,t)
     {
-      struct Epi {
-        const T* s;
-        T* t;
-        double ts, tt;
-        using Pre = T;
-        __device__ __forceinline__ Pre load(int64_t i) const { return __ldcg(s + i); }
-        __device__ __forceinline__ void operator()(int64_t i, T y, T sv) {
-          t[i] = y;
-          ts += dprod(y, sv);
-          tt += dprod(y, y);
-        }
-      } epi{V.r, V.t, 0.0, 0.0};
+      EpiTS<T> epi{V.r, V.t, 0.0, 0.0};
       spmv_range<T>(M, V.z2, sb0, sb1, epi);
       const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
@@ -508,47 +549,48 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     // pass E: x += alpha z, then x += omega z2 (the reference's two axpys,
     // fused into one pass); r = s - omega t; norms.  The best iterate is
     // saved lazily here: x still holds the previous iterate.  Each warp
-    // issues the loads of two blocks before using either.
+    // issues the loads of two chunks before using either.
     {
       double v[4] = {0.0, 0.0, 0.0, 0.0};
       constexpr int U = 2;
-      for (int64_t base = b0 + w; base < b1; base += U * kWarps) {
-        X xv[U][2];
-        T zv[U][2], z2v[U][2], sv[U][2], tv[U][2], rhv[U][2];
+      const int64_t nch = (b1 - b0 + CB - 1) / CB;
+      for (int64_t c0 = w; c0 < nch; c0 += U * kWarps) {
+        X xv[U][LV];
+        T zv[U][LV], z2v[U][LV], sv[U][LV], tv[U][LV], rhv[U][LV];
+        bool ok[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int64_t blk = base + u * kWarps;
-          if (blk < b1) {
-            const int64_t o = blk * kBLEN + lane;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              xv[u][h] = __ldcg(V.x + o + 32 * h);
-              zv[u][h] = __ldcg(V.z + o + 32 * h);
-              z2v[u][h] = __ldcg(V.z2 + o + 32 * h);
-              sv[u][h] = __ldcg(V.r + o + 32 * h);
-              tv[u][h] = __ldcg(V.t + o + 32 * h);
-              rhv[u][h] = __ldcg(V.rh + o + 32 * h);
-            }
+          const int64_t c = c0 + u * kWarps, blk = b0 + c * CB + L.bl;
+          ok[u] = c < nch && blk < b1;
+          if (ok[u]) {
+            const int64_t i0 = blk * kBLEN + L.cell0;
+            ldv<LV>(V.x + i0, xv[u]);
+            ldv<LV>(V.z + i0, zv[u]);
+            ldv<LV>(V.z2 + i0, z2v[u]);
+            ldv<LV>(V.r + i0, sv[u]);
+            ldv<LV>(V.t + i0, tv[u]);
+            ldv<LV>(V.rh + i0, rhv[u]);
           }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int64_t blk = base + u * kWarps;
-          if (blk < b1) {
-            const int64_t o = blk * kBLEN + lane;
+          if (ok[u]) {
+            const int64_t i0 = (b0 + (c0 + u * kWarps) * CB + L.bl) * kBLEN + L.cell0;
+            if (st.best_is_x) stv<LV>(V.xo + i0, xv[u]);
+            X xn[LV];
+            T rn[LV];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int64_t i = o + 32 * h;
-              if (st.best_is_x) V.xo[i] = xv[u][h];
-              const X x1 = xv[u][h] + (X)alpha * (X)zv[u][h];
-              V.x[i] = x1 + (X)omega * (X)z2v[u][h];
-              const T rn = sv[u][h] - to * tv[u][h];
-              V.r[i] = rn;
-              v[0] = nanmax(v[0], fabs((double)rn));
-              v[1] += dprod(rhv[u][h], rn);
-              v[2] += dprod(rn, rn);
-              v[3] += dprod(rhv[u][h], rhv[u][h]);
+            for (int k = 0; k < LV; ++k) {
+              const X x1 = xv[u][k] + (X)alpha * (X)zv[u][k];
+              xn[k] = x1 + (X)omega * (X)z2v[u][k];
+              rn[k] = sv[u][k] - to * tv[u][k];
+              v[0] = nanmax(v[0], fabs((double)rn[k]));
+              v[1] += dprod(rhv[u][k], rn[k]);
+              v[2] += dprod(rn[k], rn[k]);
+              v[3] += dprod(rhv[u][k], rhv[u][k]);
             }
+            stv<LV>(V.x + i0, xn);
+            stv<LV>(V.r + i0, rn);
           }
         }
       }
@@ -687,15 +729,37 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
       double* r;
       double* rh;
       double v[3];
-      using Pre = double;
-      __device__ __forceinline__ Pre load(int64_t i) const { return __ldg(b + i); }
-      __device__ __forceinline__ void operator()(int64_t i, double y, double bi) {
+      struct Pre {
+        double b[2];
+      };
+      __device__ __forceinline__ Pre load(int64_t i0) const {
+        Pre p;
+        ldv<2>(b + i0, p.b);
+        return p;
+      }
+      __device__ __forceinline__ Pre load1(int64_t i) const {
+        Pre p{};
+        p.b[0] = __ldg(b + i);
+        return p;
+      }
+      __device__ __forceinline__ double acc(double y, double bi) {
         const double rv = bi - y;
-        r[i] = rv;
-        rh[i] = rv;
         v[0] = nanmax(v[0], fabs(y));
         v[1] = nanmax(v[1], fabs(rv));
         v[2] += rv * rv;
+        return rv;
+      }
+      __device__ __forceinline__ void vec(int64_t i0, const double (&y)[2], const Pre& p) {
+        double rr[2];
+        rr[0] = acc(y[0], p.b[0]);
+        rr[1] = acc(y[1], p.b[1]);
+        stv<2>(r + i0, rr);
+        stv<2>(rh + i0, rr);
+      }
+      __device__ __forceinline__ void one(int64_t i, double y, const Pre& p, int j) {
+        const double rv = acc(y, p.b[j]);
+        r[i] = rv;
+        rh[i] = rv;
       }
     } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
     spmv_range<double>(M, pr.x, sb0, sb1, epi);
@@ -845,7 +909,8 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
   __shared__ Smem sm;
   const int team = A.team;
   const int g = blockIdx.x / team, rank = blockIdx.x % team;
-  GridBarrier B{A.bars + g, A.abort_flag, (unsigned)team, globaltimer_ns() + A.timeout_ns, 0u, nullptr, 0ull};
+  GridBarrier B{A.bars + g, A.abort_flag, (unsigned)team, globaltimer_ns() + A.timeout_ns, 0u, A.prof,
+                globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = rank;
     sm.team_size = team;
@@ -856,7 +921,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
   double* red = A.red + (size_t)g * kRedQ * team;
   while (true) {
     if (rank == 0 && threadIdx.x == 0) A.slots[g] = atomicAdd(A.queue, 1);
-    if (!B.sync(&sm.flag)) return;
+    if (!B.sync(&sm.flag, 9)) return;
     unsigned long long t_begin = 0;
     if (threadIdx.x == 0) {
       t_begin = globaltimer_ns();

@@ -419,6 +419,7 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
 int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x, cup2d_solve_stats* stats,
                                void* stream) {
   if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_b) || !aligned16(d_x)) return CUP2D_INVALID_ARGUMENT;  // 16-byte vector accesses
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   const cup2d_solve_opts& o = h->opts;
   int st;
@@ -690,6 +691,9 @@ struct cup2d_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   bool have_timeline = false;
+  DevBuf<unsigned long long> prof;  // phase timers (profiling on)
+  bool profiling = false;
+  int prof_grid = 0;
 };
 
 extern "C" {
@@ -709,6 +713,7 @@ int cup2d_batch_destroy(cup2d_batch* B) {
   B->dstats.release();
   B->P.release();
   B->P32.release();
+  B->prof.release();
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -819,7 +824,7 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
   if (!B || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
   const int n = (int)B->probs.size();
   for (int i = 0; i < n; ++i)
-    if (!d_b[i] || !d_x[i]) return CUP2D_INVALID_ARGUMENT;
+    if (!d_b[i] || !d_x[i] || !aligned16(d_b[i]) || !aligned16(d_x[i])) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const cup2d_solve_opts& o = B->opts;
   const bool mixed = o.precision == CUP2D_PREC_MIXED;
@@ -866,6 +871,17 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
   a.sp = SolveParams{o.tol_abs, o.tol_rel, o.reliable_delta, o.max_restarts, o.max_iter, o.subtract_mean,
                      o.reliable_restart};
   a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
+  a.prof = nullptr;
+  if (B->profiling) {
+    const int64_t words = (int64_t)grid * kProfPhases * 2;
+    if ((st = B->prof.ensure(words))) return st;
+    if (B->prof_grid != grid) {  // timers accumulate over launches of one grid size
+      if (cudaMemsetAsync(B->prof.p, 0, sizeof(unsigned long long) * words, s) != cudaSuccess)
+        return CUP2D_CUDA_ERROR;
+      B->prof_grid = grid;
+    }
+    a.prof = B->prof.p;
+  }
   if (stats) cudaEventRecord(B->ev0, s);
   const cudaError_t e = launch_bicgstab_batch(a, grid, mixed, s);
   if (e != cudaSuccess) return from_cuda(e);
@@ -923,6 +939,30 @@ int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x, 
                         s) != cudaSuccess)
       return CUP2D_CUDA_ERROR;
   return cudaStreamSynchronize(s) == cudaSuccess ? CUP2D_OK : CUP2D_CUDA_ERROR;
+}
+
+int cup2d_batch_set_profiling(cup2d_batch* B, int32_t enable) {
+  if (!B) return CUP2D_INVALID_ARGUMENT;
+  B->profiling = enable != 0;
+  B->prof_grid = 0;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_profile(cup2d_batch* B, double* compute_ms, double* wait_ms, int32_t nphases) {
+  if (!B || !compute_ms || !wait_ms || nphases < kProfPhases) return CUP2D_INVALID_ARGUMENT;
+  for (int q = 0; q < kProfPhases; ++q) compute_ms[q] = wait_ms[q] = 0.0;
+  if (!B->profiling || B->prof_grid <= 0) return CUP2D_OK;
+  const int g = B->prof_grid;
+  std::vector<unsigned long long> t((size_t)g * kProfPhases * 2);
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(t.data(), B->prof.p, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  for (int c = 0; c < g; ++c)
+    for (int q = 0; q < kProfPhases; ++q) {
+      compute_ms[q] += 1e-6 * (double)t[((size_t)c * kProfPhases + q) * 2] / g;
+      wait_ms[q] += 1e-6 * (double)t[((size_t)c * kProfPhases + q) * 2 + 1] / g;
+    }
+  return CUP2D_OK;
 }
 
 int cup2d_batch_timeline(const cup2d_batch* B, double* begin_ms, double* end_ms, double* launch_ms) {

@@ -9,6 +9,10 @@ namespace cup2d {
 
 constexpr int kMaxLevels = 24;
 
+// The solve kernels access vectors 16 bytes per lane: caller buffers must be
+// 16-byte aligned (cudaMalloc gives 256).
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 struct AssembleIn {
   int32_t bpdx, bpdy, level_max, periodic_x, periodic_y;
   int64_t nblocks;
@@ -187,6 +191,7 @@ struct BatchArgs {
   int* abort_flag;          // zeroed
   SolveParams sp;
   unsigned long long timeout_ns;
+  unsigned long long* prof;  // per-CTA phase timers, or null
 };
 
 constexpr int kSolveThreads = 256;

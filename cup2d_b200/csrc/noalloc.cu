@@ -90,6 +90,7 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
                                                   cup2d_solve_stats* stats, void* stream) {
   using namespace cup2d;
   if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_b) || !aligned16(d_x)) return CUP2D_INVALID_ARGUMENT;  // 16-byte vector accesses
   HandleView v;
   if (handle_view(h, &v) != CUP2D_OK) return CUP2D_INVALID_ARGUMENT;
   if (v.nb > kNoAllocMaxBlocks) return CUP2D_INVALID_ARGUMENT;  // beyond the static scratch

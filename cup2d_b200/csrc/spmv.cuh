@@ -128,54 +128,196 @@ __device__ __forceinline__ void spmv_block(const MeshView& M, int64_t blk, const
   }
 }
 
-// y = A z over blocks [b0, b1) by the whole CTA.  The epilogue is a functor
-// with `Pre load(i)`, the operands it needs at cell i (loaded together with
-// the gather, before y is known), and `operator()(i, y, pre)`, called once
-// per cell by the thread that computed it, in no particular order.  The
-// neighbour tables of a warp's next block pair are fetched while it
-// computes the current pair, so each pair costs one round trip to memory.
+// ------------------------------------------------ 16-byte lane layout ----
+//
+// The range passes move 16 bytes per lane and access: V = 4 consecutive
+// cells of a row for FP32 (a warp covers two blocks, 16 lanes each), V = 2
+// for FP64 (a warp covers one block).  A "chunk" is the CB blocks one warp
+// access covers.  Lane l of a chunk owns cells cell0 .. cell0 + V - 1 of
+// block bl, row iy; in-row neighbours of other lanes and the rows above and
+// below come from shuffles, cells across a block face from the neighbour.
+
+template <class T>
+struct Lane {
+  static constexpr int V = 16 / (int)sizeof(T);  // cells per lane
+  static constexpr int LB = kBLEN / V;           // lanes per block
+  static constexpr int LR = kBS / V;             // lanes per row
+  static constexpr int CB = 32 / LB;             // blocks per chunk
+  int sub, bl, iy, ix0, cell0;
+  __device__ __forceinline__ explicit Lane(int lane) {
+    sub = lane % LB;
+    bl = lane / LB;
+    iy = sub / LR;
+    ix0 = V * (sub % LR);
+    cell0 = iy * kBS + ix0;
+  }
+};
+
+// N consecutive values at p (N * sizeof(T) a multiple of 8 bytes, p aligned
+// to it): ld.global.cg / plain stores of 8- or 16-byte vectors.
+template <int N, class T>
+__device__ __forceinline__ void ldv(const T* p, T (&v)[N]) {
+  static_assert(N * sizeof(T) % 8 == 0, "vector size");
+  if constexpr (sizeof(T) == 4 && N == 2) {
+    const float2 a = __ldcg(reinterpret_cast<const float2*>(p));
+    v[0] = a.x; v[1] = a.y;
+  } else if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int k = 0; k < N; k += 4) {
+      const float4 a = __ldcg(reinterpret_cast<const float4*>(p + k));
+      v[k] = a.x; v[k + 1] = a.y; v[k + 2] = a.z; v[k + 3] = a.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k += 2) {
+      const double2 a = __ldcg(reinterpret_cast<const double2*>(p + k));
+      v[k] = a.x; v[k + 1] = a.y;
+    }
+  }
+}
+
+template <int N, class T>
+__device__ __forceinline__ void stv(T* p, const T (&v)[N]) {
+  static_assert(N * sizeof(T) % 8 == 0, "vector size");
+  if constexpr (sizeof(T) == 4 && N == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int k = 0; k < N; k += 4)
+      *reinterpret_cast<float4*>(p + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k += 2) *reinterpret_cast<double2*>(p + k) = make_double2(v[k], v[k + 1]);
+  }
+}
+
+template <class T>
+struct ChunkGather {
+  static constexpr int V = Lane<T>::V;
+  int4 nb;
+  T z[V];         // this lane's cells
+  T xm, xp;       // across the x faces (first / last lane of a row)
+  T ym[V], yp[V]; // across the y faces (rows 0 / 7)
+};
+
+template <class T>
+__device__ __forceinline__ void gather_chunk(const int4& nb, int64_t blk, bool valid, const T* __restrict__ z,
+                                             const Lane<T>& L, ChunkGather<T>& g) {
+  constexpr int V = Lane<T>::V;
+  g.nb = nb;
+  g.xm = g.xp = T(0);
+#pragma unroll
+  for (int j = 0; j < V; ++j) g.z[j] = g.ym[j] = g.yp[j] = T(0);
+  if (!valid) return;
+  ldv<V>(z + blk * kBLEN + L.cell0, g.z);
+  if (L.ix0 == 0 && nb.x >= 0) g.xm = ldcg(z + (int64_t)nb.x * kBLEN + L.iy * kBS + (kBS - 1));
+  if (L.ix0 + V == kBS && nb.y >= 0) g.xp = ldcg(z + (int64_t)nb.y * kBLEN + L.iy * kBS);
+  if (L.iy == 0 && nb.z >= 0) ldv<V>(z + (int64_t)nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
+  if (L.iy == kBS - 1 && nb.w >= 0) ldv<V>(z + (int64_t)nb.w * kBLEN + L.ix0, g.yp);
+}
+
+// Stencil rows of the lane's cells, summed left, right, below, above as the
+// assembled rows are (explicit rows get meaningless values).  All lanes of
+// the warp take part (shuffles).
+template <class T>
+__device__ __forceinline__ void stencil_chunk(const ChunkGather<T>& g, const Lane<T>& L, T (&y)[Lane<T>::V]) {
+  constexpr int V = Lane<T>::V, LR = Lane<T>::LR;
+  const T from_l = __shfl_up_sync(kFull, g.z[V - 1], 1);
+  const T from_r = __shfl_down_sync(kFull, g.z[0], 1);
+  T dn[V], up[V];
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    dn[j] = __shfl_up_sync(kFull, g.z[j], LR);
+    up[j] = __shfl_down_sync(kFull, g.z[j], LR);
+  }
+  const bool left_in = (L.sub % LR) > 0, right_in = (L.sub % LR) < LR - 1;
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    T a = T(0);
+    int n = 0;
+    if (j > 0) { a += g.z[j - 1]; n++; }
+    else if (left_in) { a += from_l; n++; }
+    else if (g.nb.x >= 0) { a += g.xm; n++; }
+    if (j < V - 1) { a += g.z[j + 1]; n++; }
+    else if (right_in) { a += from_r; n++; }
+    else if (g.nb.y >= 0) { a += g.xp; n++; }
+    if (L.iy > 0) { a += dn[j]; n++; }
+    else if (g.nb.z >= 0) { a += g.ym[j]; n++; }
+    if (L.iy < kBS - 1) { a += up[j]; n++; }
+    else if (g.nb.w >= 0) { a += g.yp[j]; n++; }
+    y[j] = a - T(n) * g.z[j];
+  }
+}
+
+// y = A z over blocks [b0, b1) by the whole CTA, in the 16-byte layout.  The
+// epilogue functor provides
+//   Pre load(i0) / Pre load1(i)  operands of the lane's V cells from i0 (or
+//                                of one cell i, as element 0), loaded with
+//                                the gather, before y is known;
+//   vec(i0, y[V], pre)           the V cells (all stencil rows);
+//   one(i, y, pre, j)            cell i, element j of pre (lanes owning an
+//                                explicit row, and the explicit rows);
+// each cell is handed over exactly once, by one thread, in no particular
+// order.  A warp has two chunks in flight, and fetches the neighbour tables
+// of its next two chunks while it computes the current ones.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int64_t b0, int64_t b1,
                                            Epi& epi) {
   using Pre = typename Epi::Pre;
+  constexpr int V = Lane<T>::V, CB = Lane<T>::CB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  int64_t blk = b0 + w;
-  int4 na = make_int4(0, 0, 0, 0), nbb = make_int4(0, 0, 0, 0);
-  if (blk < b1) na = block_nbr(M, blk);
-  if (blk + nw < b1) nbb = block_nbr(M, blk + nw);
-  for (; blk < b1; blk += 2 * nw) {
-    const bool two = blk + nw < b1;  // warp-uniform
-    BlockGather<T> ga, gb;
-    gather_block_nb<T>(na, blk, z, lane, ga);
-    const int64_t oa = blk * kBLEN, ob = (blk + nw) * kBLEN;
-    const Pre pa0 = epi.load(oa + lane), pa1 = epi.load(oa + lane + 32);
-    Pre pb0{}, pb1{};
-    if (two) {
-      gather_block_nb<T>(nbb, blk + nw, z, lane, gb);
-      pb0 = epi.load(ob + lane);
-      pb1 = epi.load(ob + lane + 32);
+  const Lane<T> L(lane);
+  const int64_t nch = (b1 - b0 + CB - 1) / CB;
+  auto block_of = [&](int64_t c) { return b0 + c * CB + L.bl; };
+  auto nbr_of = [&](int64_t c) {
+    const int64_t blk = block_of(c);
+    return (c < nch && blk < b1) ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
+  };
+  int64_t c = w;
+  int4 na = nbr_of(c), nbb = nbr_of(c + nw);
+  for (; c < nch; c += 2 * nw) {
+    const int64_t ca = c, cb = c + nw;
+    const int64_t ba = block_of(ca), bb = block_of(cb);
+    const bool va = ba < b1, vb = cb < nch && bb < b1;
+    ChunkGather<T> ga, gb;
+    gather_chunk<T>(na, ba, va, z, L, ga);
+    gather_chunk<T>(nbb, bb, vb, z, L, gb);
+    const int64_t ia = ba * kBLEN + L.cell0, ib = bb * kBLEN + L.cell0;
+    Pre pa{}, pb{};
+    if (va) pa = epi.load(ia);
+    if (vb) pb = epi.load(ib);
+    na = nbr_of(c + 2 * nw);
+    nbb = nbr_of(c + 3 * nw);
+    T y[V];
+    stencil_chunk<T>(ga, L, y);
+    if (va) {
+      const unsigned mk = (unsigned)(explicit_mask<T>(M, ba, ga.nb) >> L.cell0) & ((1u << V) - 1u);
+      if (mk == 0u) {
+        epi.vec(ia, y, pa);
+      } else {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+          if (!((mk >> j) & 1u)) epi.one(ia + j, y[j], pa, j);
+      }
     }
-    const int64_t nxt = blk + 2 * nw;
-    if (nxt < b1) na = block_nbr(M, nxt);
-    if (nxt + nw < b1) nbb = block_nbr(M, nxt + nw);
-    T y0, y1;
-    stencil_block<T>(ga, lane, y0, y1);
-    unsigned long long m = explicit_mask<T>(M, blk, ga.nb);
-    if (!((m >> lane) & 1ull)) epi(oa + lane, y0, pa0);
-    if (!((m >> (lane + 32)) & 1ull)) epi(oa + lane + 32, y1, pa1);
-    if (two) {
-      stencil_block<T>(gb, lane, y0, y1);
-      m = explicit_mask<T>(M, blk + nw, gb.nb);
-      if (!((m >> lane) & 1ull)) epi(ob + lane, y0, pb0);
-      if (!((m >> (lane + 32)) & 1ull)) epi(ob + lane + 32, y1, pb1);
+    stencil_chunk<T>(gb, L, y);
+    if (vb) {
+      const unsigned mk = (unsigned)(explicit_mask<T>(M, bb, gb.nb) >> L.cell0) & ((1u << V) - 1u);
+      if (mk == 0u) {
+        epi.vec(ib, y, pb);
+      } else {
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+          if (!((mk >> j) & 1u)) epi.one(ib + j, y[j], pb, j);
+      }
     }
   }
   if (b1 > b0) {
     const int r0 = __ldg(M.xbase + b0), r1 = __ldg(M.xbase + b1);
     for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
       const int64_t i = (int64_t)__ldg(M.rowcell + r);
-      const Pre pre = epi.load(i);
-      epi(i, explicit_row<T>(M, r, z), pre);
+      const Pre pre = epi.load1(i);
+      epi.one(i, explicit_row<T>(M, r, z), pre, 0);
     }
   }
 }

@@ -173,8 +173,8 @@ class Solver:
                 "cup2d_poisson_export_csr")
         return rp, col, val
 
-    PHASES = ("residual/init", "A: p, P^-1", "B: SpMV (rhat,nu)", "C: x, s, P^-1", "D: SpMV (t,s),(t,t)",
-              "E: x, r, norms", "true residual", "mean removal", "sum b", "unused")
+    PHASES = ("residual/init", "A: p, P^-1", "B: SpMV (rhat,nu)", "C: s, P^-1", "D: SpMV (t,s),(t,t)",
+              "E: x, r, norms", "true residual", "mean removal", "sum b", "next problem")
 
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.lib().cup2d_poisson_set_profiling(self._h, int(bool(enable))), "set_profiling")
@@ -276,6 +276,17 @@ class BatchSolver:
         L.check(L.lib().cup2d_batch_solve(self._h, pb, px, st), "cup2d_batch_solve")
         self.last_stats = [s.as_dict() for s in st]
         return self.last_stats
+
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(L.lib().cup2d_batch_set_profiling(self._h, int(bool(enable))), "cup2d_batch_set_profiling")
+
+    def profile(self) -> dict:
+        """Per-phase (compute ms, barrier-wait ms), per-CTA averages over the
+        launches since profiling was enabled (phases as Solver.PHASES)."""
+        c = np.zeros(10)
+        w = np.zeros(10)
+        L.check(L.lib().cup2d_batch_profile(self._h, _pd(c), _pd(w), 10), "cup2d_batch_profile")
+        return {name: (float(c[i]), float(w[i])) for i, name in enumerate(Solver.PHASES) if c[i] or w[i]}
 
     def timeline(self) -> tuple[np.ndarray, np.ndarray, float]:
         """(begin_ms, end_ms, launch_ms) of the last solve that returned stats."""

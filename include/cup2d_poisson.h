@@ -19,8 +19,9 @@
  *     the order of the forest passed at creation (CUP2D's blockID order).
  *   - Every entry point returns a cup2d_status; none exits or aborts.
  *   - A handle is not thread-safe; it runs its work on one CUDA stream.
- *   - Pointers named d_* are device pointers on the handle's device; the
- *     others are host pointers.  `stream` is a cudaStream_t used as given
+ *   - Pointers named d_* are device pointers on the handle's device, 16-byte
+ *     aligned for the solves (cudaMalloc gives 256); the others are host
+ *     pointers.  `stream` is a cudaStream_t used as given
  *     (NULL is the legacy default stream, as in the CUDA runtime).  The
  *     host-buffer solve runs on the handle's own stream.
  */
@@ -201,6 +202,11 @@ int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x,
  * took it and finished it, in ms from the first start, and the launch's
  * duration (CUDA events); for tuning the team size. */
 int cup2d_batch_timeline(const cup2d_batch* B, double* begin_ms, double* end_ms, double* launch_ms);
+/* Per-phase device timers of batched launches, as cup2d_poisson_profile
+ * (per-CTA averages in ms since enabling); phase 9 is the wait for the next
+ * problem of the queue. */
+int cup2d_batch_set_profiling(cup2d_batch* B, int32_t enable);
+int cup2d_batch_profile(cup2d_batch* B, double* compute_ms, double* wait_ms, int32_t nphases);
 int cup2d_batch_destroy(cup2d_batch* B);
 
 /* ------------------------------------------------- synthetic problems ---- */
