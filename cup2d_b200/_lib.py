@@ -60,6 +60,7 @@ SIGNATURES = {
     "cup2d_poisson_solve_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.POINTER(SolveStats), C.c_void_p]),
     "cup2d_poisson_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cup2d_poisson_apply32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_export_csr": (C.c_int, [C.c_void_p, P_i64, P_i64, P_i64, P_i32, P_f64]),

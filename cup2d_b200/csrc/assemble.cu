@@ -217,13 +217,6 @@ __global__ void k_classify(ForestDev F, int32_t* __restrict__ nbr, unsigned long
   hblk[b] = h0 / (double)(1ll << l);
 }
 
-// SpMV cost of each block: the stencil rows plus one per explicit row; its
-// prefix sum partitions the SpMV passes across CTAs.
-__global__ void k_spmv_cost(const int32_t* __restrict__ xcount, int64_t nb, int32_t* __restrict__ w) {
-  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (b < nb) w[b] = kSpmvBlockCost + xcount[b];
-}
-
 // ------------------------------------------------------------- scans ------
 
 // Exclusive scan of int32 counts into int32 offsets (out[n] = total), in
@@ -535,8 +528,6 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   k_fill_tables<<<g, 256, 0, s>>>(F, out.table, out.err);
   k_classify<<<g, 256, 0, s>>>(F, out.nbr, out.xmask, out.xcount, out.hblk, in.h0, out.err);
   launch_exclusive_scan(out.xcount, nb, out.xbase, out.scan_tmp, s);
-  k_spmv_cost<<<g, 256, 0, s>>>(out.xcount, nb, out.wcost);
-  launch_exclusive_scan(out.wcost, nb, out.wprefix, out.scan_tmp, s);
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
   int32_t hR = 0;
   int herr = 0;

@@ -10,7 +10,8 @@
 // The reference runs each iteration as ~25 library launches (cuSPARSE COO
 // SpMV, cuBLAS dot/nrm2/axpy/scal/Idamax/Dgemm), 8 one-thread scalar kernels
 // and 4 host round-trips.  Here one cooperative kernel runs the whole solve.
-// Each CTA owns a contiguous range of blocks; an iteration is five fused
+// Each CTA owns an equal contiguous range of blocks, and an equal share of
+// the explicit (coarse/fine) rows for the SpMVs; an iteration is five fused
 // passes over them, separated by bounded grid barriers:
 //
 //   A  p = r + beta (p - omega nu);  z = P^-1 p          (R r,p,nu  W p,z)
@@ -87,7 +88,6 @@ struct Smem {
   // the CTAs solving one problem together: this CTA's rank among them and
   // their number (the whole grid for a single solve, a group in a batch)
   int team_rank, team_size;
-  int64_t bounds[2];  // batch: this CTA's SpMV block range of the current problem
   int slot;           // batch: the problem the team works on
 };
 
@@ -348,7 +348,7 @@ struct EpiTS {
 __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
                                               double mean_b, const double* __restrict__ x, float* __restrict__ r,
                                               float* __restrict__ rh, bool set_rh, double* __restrict__ red,
-                                              int64_t sb0, int64_t sb1) {
+                                              int64_t b0, int64_t b1, int64_t r0, int64_t r1) {
   struct Epi {
     const double* b;
     double mean_b;
@@ -397,7 +397,7 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       if (set_rh) rh[i] = r32;
     }
   } epi{b, mean_b, r, rh, set_rh, {0.0, 0.0, 0.0, 0.0, 0.0}};
-  spmv_range<double>(M, x, sb0, sb1, epi);
+  spmv_range<double>(M, x, b0, b1, r0, r1, epi);
   cta_partials<5>(sm, epi.v, 0x11u, red, Q_RU);
 }
 
@@ -416,7 +416,7 @@ struct MixedCtx {  // what the reliable update needs
 template <class T, class X, bool RU>
 __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const Pinv<T>& pin,
                               const Vecs<T, X> V, double* __restrict__ red, int64_t b0, int64_t b1,
-                              int64_t sb0, int64_t sb1, double tol_abs, double tol_rel, int max_restarts,
+                              int64_t r0, int64_t r1, double tol_abs, double tol_rel, int max_restarts,
                               int max_iter, const MixedCtx& mx, IterState& st) {
   constexpr int TB = Pinv<T>::kTile;
   constexpr int LV = Lane<T>::V, CB = Lane<T>::CB;  // 16-byte lane layout
@@ -492,7 +492,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     // pass B: nu = A z; (rhat, nu)
     {
       EpiRhNu<T> epi{V.rh, V.nu, 0.0};
-      spmv_range<T>(M, V.z, sb0, sb1, epi);
+      spmv_range<T>(M, V.z, b0, b1, r0, r1, epi);
       const double v[1] = {epi.acc};
       cta_partials<1>(sm, v, 0u, red, Q_RHNU);
     }
@@ -538,7 +538,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     // pass D: t = A z2; (t,s), (t,t)
     {
       EpiTS<T> epi{V.r, V.t, 0.0, 0.0};
-      spmv_range<T>(M, V.z2, sb0, sb1, epi);
+      spmv_range<T>(M, V.z2, b0, b1, r0, r1, epi);
       const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
     }
@@ -617,7 +617,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       if (claims || sqrt(nr) < mx.delta * rmax_since || since >= kMaxSweep) {
         since = 0;
         // pass E's barrier already ordered every CTA's x update before this
-        true_residual(sm, M, mx.b, mx.mean_b, V.x, V.r, V.rh, mx.restart, red, sb0, sb1);
+        true_residual(sm, M, mx.b, mx.mean_b, V.x, V.r, V.rh, mx.restart, red, b0, b1, r0, r1);
         if (!B.sync(&sm.flag, 6)) return false;
         grid_reduce<5>(sm, 0x11u, red, Q_RU);
         ++st.updates;
@@ -716,10 +716,10 @@ __device__ __forceinline__ void write_stats(const Smem& sm, DevStats* stats, con
 
 // Plain FP64 solve of one problem by the team: BiCGSTABSolver::main
 // (BiCGSTAB.cu:412-620) and the mean removal (ExpAMRSolver.cpp:383-415).
-// [b0,b1) is this CTA's block range, [sb0,sb1) its SpMV range.
+// [b0,b1) is this CTA's block range, [r0,r1) its explicit rows.
 __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
-                           const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
-                           int64_t sb1) {
+                           const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t r0,
+                           int64_t r1) {
   const MeshView& M = pr.M;
   const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
@@ -762,7 +762,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
         rh[i] = rv;
       }
     } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
-    spmv_range<double>(M, pr.x, sb0, sb1, epi);
+    spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi);
     cta_partials<3>(sm, epi.v, 0x3u, red, Q_INIT);
   }
   if (!B.sync(&sm.flag, 0)) return false;
@@ -779,7 +779,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
   const MixedCtx none{};
-  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, red, b0, b1, sb0, sb1, sp.tol_abs, sp.tol_rel,
+  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, red, b0, b1, r0, r1, sp.tol_abs, sp.tol_rel,
                                             sp.max_restarts, sp.max_iter, none, st))
     return false;
   take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
@@ -790,8 +790,8 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
 
 // Mixed-precision solve of one problem by the team.
 __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, const ProblemMixed& pr,
-                            const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t sb0,
-                            int64_t sb1) {
+                            const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t r0,
+                            int64_t r1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // Neumann compatibility: project b to zero sum (sum b / n)
@@ -812,7 +812,7 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
   mx.tol_abs = sp.tol_abs;
   mx.tol_rel = sp.tol_rel;
   mx.restart = sp.reliable_restart != 0;
-  true_residual(sm, pr.M, pr.b, mx.mean_b, pr.x, pr.r, pr.rh, true, red, sb0, sb1);
+  true_residual(sm, pr.M, pr.b, mx.mean_b, pr.x, pr.r, pr.rh, true, red, b0, b1, r0, r1);
   if (!B.sync(&sm.flag, 0)) return false;
   grid_reduce<5>(sm, 0x11u, red, Q_RU);
   IterState st;
@@ -830,7 +830,7 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
   const bool done0 = st.err_true <= sp.tol_abs || st.err_true == 0.0;
   if (done0) {
     st.status = CUP2D_OK;
-  } else if (!bicgstab_loop<float, double, true>(sm, B, pr.M, pin, V, red, b0, b1, sb0, sb1, sp.tol_abs,
+  } else if (!bicgstab_loop<float, double, true>(sm, B, pr.M, pin, V, red, b0, b1, r0, r1, sp.tol_abs,
                                                  sp.tol_rel, sp.max_restarts, sp.max_iter, mx, st)) {
     return false;
   }
@@ -838,17 +838,6 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
   if (sp.subtract_mean && !subtract_mean(sm, B, pr.M, pr.x, red, b0, b1)) return false;
   write_stats(sm, pr.stats, st, st.updates, st.status == CUP2D_OK ? st.err_true : st.err_opt, 0.0);
   return true;
-}
-
-// first b in [0, nb] with wp[b] >= target (wp strictly increasing)
-__device__ __forceinline__ int64_t cost_lower_bound(const int32_t* __restrict__ wp, int64_t nb, int64_t target) {
-  int64_t lo = 0, hi = nb;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if ((int64_t)__ldg(wp + mid) < target) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
 }
 
 }  // namespace
@@ -862,7 +851,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
   __shared__ Smem sm;
   const int64_t nb = S.M.nb;
   const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  const int64_t r0 = S.M.R * blockIdx.x / gridDim.x, r1 = S.M.R * (blockIdx.x + 1) / gridDim.x;
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -873,14 +862,14 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
   __syncthreads();
   const Problem64 pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
   const SolveParams sp{S.tol_abs, S.tol_rel, 0.0, S.max_restarts, S.max_iter, S.subtract_mean, 0};
-  solve_fp64(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
+  solve_fp64(sm, B, pin, pr, sp, S.red, b0, b1, r0, r1);
 }
 
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
   __shared__ Smem sm;
   const int64_t nb = S.M.nb;
   const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t sb0 = __ldg(S.sbounds + blockIdx.x), sb1 = __ldg(S.sbounds + blockIdx.x + 1);
+  const int64_t r0 = S.M.R * blockIdx.x / gridDim.x, r1 = S.M.R * (blockIdx.x + 1) / gridDim.x;
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -892,7 +881,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   const ProblemMixed pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
   const SolveParams sp{S.tol_abs, S.tol_rel, S.reliable_delta, S.max_restarts, S.max_iter, S.subtract_mean,
                        S.reliable_restart};
-  solve_mixed(sm, B, pin, pr, sp, S.red, b0, b1, sb0, sb1);
+  solve_mixed(sm, B, pin, pr, sp, S.red, b0, b1, r0, r1);
 }
 
 // ========================================================= batches ========
@@ -925,30 +914,23 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
     unsigned long long t_begin = 0;
     if (threadIdx.x == 0) {
       t_begin = globaltimer_ns();
-      const int q = __ldcg(A.slots + g);
-      sm.slot = q;
-      if (q < A.nprob) {
-        const int p = __ldg(A.order + q);
-        const MeshView& M = MIXED ? A.pmx[p].M : A.p64[p].M;
-        const int64_t W = __ldg(M.wprefix + M.nb);
-        sm.bounds[0] = cost_lower_bound(M.wprefix, M.nb, W * rank / team);
-        sm.bounds[1] = rank == team - 1 ? M.nb : cost_lower_bound(M.wprefix, M.nb, W * (rank + 1) / team);
-      }
+      sm.slot = __ldcg(A.slots + g);
     }
     __syncthreads();
     const int q = sm.slot;
     if (q >= A.nprob) return;
     const int p = __ldg(A.order + q);
-    const int64_t sb0 = sm.bounds[0], sb1 = sm.bounds[1];
     bool ok;
     if constexpr (MIXED) {
       const ProblemMixed pr = A.pmx[p];
       const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
-      ok = solve_mixed(sm, B, pin, pr, A.sp, red, b0, b1, sb0, sb1);
+      const int64_t r0 = pr.M.R * rank / team, r1 = pr.M.R * (rank + 1) / team;
+      ok = solve_mixed(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     } else {
       const Problem64 pr = A.p64[p];
       const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
-      ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, sb0, sb1);
+      const int64_t r0 = pr.M.R * rank / team, r1 = pr.M.R * (rank + 1) / team;
+      ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     }
     if (!ok) return;
     if (rank == 0 && threadIdx.x == 0) {
@@ -1003,23 +985,41 @@ cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cuda
 
 // ------------------------------------------------------- single ops -------
 
-__global__ void __launch_bounds__(256) k_spmv64(MeshView M, const double* __restrict__ x, double* __restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t blk = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); blk < M.nb; blk += warps) {
-    const int64_t o = blk * kBLEN;
-    double y0, y1;
-    spmv_block<double>(M, blk, x, lane, y0, y1);
-    y[o + lane] = y0;
-    y[o + lane + 32] = y1;
-  }
+// y = A x with the solver's own SpMV (the range form of the passes): CTA c
+// takes an equal share of the blocks and of the explicit rows.
+template <class T>
+struct EpiY {
+  static constexpr int LV = Lane<T>::V;
+  T* y;
+  struct Pre {};
+  __device__ __forceinline__ Pre load(int64_t) const { return Pre{}; }
+  __device__ __forceinline__ Pre load1(int64_t) const { return Pre{}; }
+  __device__ __forceinline__ void vec(int64_t i0, const T (&v)[LV], const Pre&) { stv<LV>(y + i0, v); }
+  __device__ __forceinline__ void one(int64_t i, T v, const Pre&, int) { y[i] = v; }
+};
+
+template <class T>
+__global__ void __launch_bounds__(kSolveThreads) k_apply(MeshView M, const T* __restrict__ x, T* __restrict__ y) {
+  const int64_t b0 = M.nb * blockIdx.x / gridDim.x, b1 = M.nb * (blockIdx.x + 1) / gridDim.x;
+  const int64_t r0 = M.R * blockIdx.x / gridDim.x, r1 = M.R * (blockIdx.x + 1) / gridDim.x;
+  EpiY<T> epi{y};
+  spmv_range<T>(M, x, b0, b1, r0, r1, epi);
+}
+
+template <class T>
+cudaError_t launch_apply(const MeshView& M, const T* x, T* y, cudaStream_t s) {
+  if (M.nb <= 0) return cudaSuccess;
+  const int64_t ctas = (M.nb + 15) / 16;
+  k_apply<T><<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(M, x, y);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s) {
-  if (M.nb <= 0) return cudaSuccess;
-  const int64_t ctas = (M.nb + 7) / 8;
-  k_spmv64<<<(unsigned)(ctas < 65535 ? ctas : 65535), 256, 0, s>>>(M, x, y);
-  return cudaGetLastError();
+  return launch_apply<double>(M, x, y, s);
+}
+
+cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, cudaStream_t s) {
+  return launch_apply<float>(M, x, y, s);
 }
 
 __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int64_t nb,

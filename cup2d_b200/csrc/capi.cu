@@ -80,7 +80,7 @@ struct cup2d_poisson {
   double extent = 1.0;
   int64_t nb = 0;
   // operator
-  DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol, wcost, wprefix, rowcell;
+  DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol, rowcell;
   DevBuf<unsigned long long> xmask;
   DevBuf<double> hblk, xval, P;
   DevBuf<float> xval32, P32;
@@ -96,12 +96,7 @@ struct cup2d_poisson {
   DevBuf<int> abort_flag;
   DevBuf<DevStats> dstats;
   DevBuf<unsigned long long> prof;  // phase timers (profiling on)
-  // SpMV partition: cost prefix of the current mesh and ranges per grid
-  std::vector<int32_t> wprefix_host;
-  std::vector<int32_t> sbounds_host;
-  DevBuf<int32_t> sbounds;
-  int sb_grid = 0;
-  uint64_t mesh_version = 0, sb_version = ~0ull;
+  uint64_t mesh_version = 0;
   bool profiling = false;
   int prof_grid = 0;                // grid of the profiled solves
   DevStats* hstats = nullptr;  // pinned
@@ -165,8 +160,7 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb)) ||
       (st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
       (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
-      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)) ||
-      (st = h->wcost.ensure(nb)) || (st = h->wprefix.ensure(nb + 1)))
+      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
     return st;
   // Krylov vectors
   if ((st = h->xo.ensure(n)) || (st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) ||
@@ -189,8 +183,6 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   m.xcount = h->xcount.p;
   m.xbase = h->xbase.p;
   m.hblk = h->hblk.p;
-  m.wcost = h->wcost.p;
-  m.wprefix = h->wprefix.p;
   m.scan_tmp = h->scan_tmp.p;
   m.err = h->err.p;
   m.ctx = h;
@@ -202,11 +194,6 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
                 f->extent / ((double)std::max(f->bpdx, f->bpdy) * 8.0)};
   st = assemble_on_device(in, m, s);
   if (st) return st;
-  h->wprefix_host.resize(nb + 1);
-  if (cudaMemcpyAsync(h->wprefix_host.data(), h->wprefix.p, sizeof(int32_t) * (nb + 1), cudaMemcpyDeviceToHost, s) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
   ++h->mesh_version;
   h->bpdx = f->bpdx;
   h->bpdy = f->bpdy;
@@ -224,29 +211,6 @@ int ensure_scratch(cup2d_poisson* h) {
   if ((st = h->red.ensure((int64_t)kRedQ * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
       (st = h->abort_flag.ensure(1)) || (st = h->dstats.ensure(1)))
     return st;
-  return CUP2D_OK;
-}
-
-// Block ranges of the SpMV passes for `grid` CTAs: CTA c takes the blocks
-// whose cost prefix falls in [W*c/grid, W*(c+1)/grid).
-int ensure_sbounds(cup2d_poisson* h, int grid, cudaStream_t s) {
-  if (h->sb_grid == grid && h->sb_version == h->mesh_version) return CUP2D_OK;
-  int st = h->sbounds.ensure(grid + 1);
-  if (st) return st;
-  const std::vector<int32_t>& wp = h->wprefix_host;
-  const int64_t W = wp.back();
-  h->sbounds_host.resize(grid + 1);
-  for (int c = 0; c <= grid; ++c) {
-    const int64_t target = W * c / grid;
-    h->sbounds_host[c] = (int32_t)(std::lower_bound(wp.begin(), wp.end(), (int32_t)target) - wp.begin());
-  }
-  h->sbounds_host[grid] = (int32_t)h->nb;
-  if (cudaMemcpyAsync(h->sbounds.p, h->sbounds_host.data(), sizeof(int32_t) * (grid + 1), cudaMemcpyHostToDevice,
-                      s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  h->sb_grid = grid;
-  h->sb_version = h->mesh_version;
   return CUP2D_OK;
 }
 
@@ -392,7 +356,7 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   if (!h) return CUP2D_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   DevBuf<int32_t>* i32[] = {&h->level, &h->bx, &h->by, &h->table, &h->nbr, &h->xcount, &h->xbase,
-                            &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol, &h->wcost, &h->wprefix,
+                            &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol,
                             &h->rowcell};
   for (auto* b : i32) b->release();
   h->xmask.release();
@@ -407,7 +371,6 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   h->abort_flag.release();
   h->dstats.release();
   h->prof.release();
-  h->sbounds.release();
   if (h->hstats) cudaFreeHost(h->hstats);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -432,7 +395,6 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
   const int grid = o.precision == CUP2D_PREC_MIXED ? h->grid_for(h->gridmx) : h->grid_for(h->grid64);
   const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
-  if ((st = ensure_sbounds(h, grid, s))) return st;
   unsigned long long* prof = nullptr;
   if (h->profiling) {
     const int64_t words = (int64_t)grid * kProfPhases * 2;
@@ -474,7 +436,6 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.subtract_mean = o.subtract_mean;
     a.timeout_ns = tns;
     a.prof = prof;
-    a.sbounds = h->sbounds.p;
     e = launch_bicgstab_mixed(a, grid, s);
   } else {
     SolveArgs64 a{};
@@ -501,7 +462,6 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.subtract_mean = o.subtract_mean;
     a.timeout_ns = tns;
     a.prof = prof;
-    a.sbounds = h->sbounds.p;
     e = launch_bicgstab64(a, grid, s);
   }
   if (e != cudaSuccess) return from_cuda(e);
@@ -537,9 +497,15 @@ int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x, cup2d_solv
 }
 
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream) {
-  if (!h || !d_x || !d_y) return CUP2D_INVALID_ARGUMENT;
+  if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, s));
+}
+
+int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream) {
+  if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+  return from_cuda(launch_spmv32(h->mesh.view(), d_x, d_y, s));
 }
 
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream) {
@@ -990,7 +956,6 @@ int handle_view(const cup2d_poisson* h, HandleView* out) {
   out->nb = h->nb;
   out->grid = h->grid_for(h->grid64);
   out->opts = h->opts;
-  out->wprefix = &h->wprefix_host;
   out->ev0 = h->ev0;
   out->ev1 = h->ev1;
   return CUP2D_OK;

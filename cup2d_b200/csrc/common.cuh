@@ -33,12 +33,8 @@ struct MeshView {
   const float* __restrict__ xval32;
   const double* __restrict__ hblk;     // cell size per block
   const int32_t* __restrict__ rowcell; // [R] cell index of each explicit row
-  const int32_t* __restrict__ wprefix; // [nb+1] prefix sum of SpMV cost weights
+  int64_t R;                           // explicit rows
 };
-
-// SpMV cost weight of a block: its 64 stencil rows count as kSpmvBlockCost,
-// each explicit (coarse/fine) row adds one.
-constexpr int32_t kSpmvBlockCost = 32;
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;

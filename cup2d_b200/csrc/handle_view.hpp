@@ -17,7 +17,6 @@ struct HandleView {
   int64_t nb;                              // blocks
   int grid;                                // CTAs the FP64 solve would use
   cup2d_solve_opts opts;
-  const std::vector<int32_t>* wprefix;     // SpMV cost prefix (host copy)
   cudaEvent_t ev0, ev1;                    // the handle's timing events
 };
 

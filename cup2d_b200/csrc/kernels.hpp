@@ -36,8 +36,6 @@ struct DeviceMesh {
   int32_t* scan_tmp = nullptr;
   int* err = nullptr;
   int64_t R = 0, nnz = 0;
-  int32_t* wcost = nullptr;       // [nb] SpMV cost weights
-  int32_t* wprefix = nullptr;     // [nb+1]
   int32_t* rowlen = nullptr;      // [R]
   int32_t* rowcell = nullptr;     // [R]
   int32_t* xptr = nullptr;        // [R+1]
@@ -59,7 +57,7 @@ struct DeviceMesh {
     v.xval = xval;
     v.xval32 = xval32;
     v.rowcell = rowcell;
-    v.wprefix = wprefix;
+    v.R = R;
     v.hblk = hblk;
     return v;
   }
@@ -109,7 +107,6 @@ struct SolveArgs64 {
   int max_restarts, max_iter, subtract_mean;
   unsigned long long timeout_ns;
   unsigned long long* prof;  // per-CTA phase timers, or null
-  const int32_t* sbounds;    // [grid+1] SpMV block ranges, balanced by cost
 };
 
 // Mixed precision: FP32 Krylov vectors, FP64 solution and true residual.
@@ -134,7 +131,6 @@ struct SolveArgsMixed {
   int max_restarts, max_iter, subtract_mean, reliable_restart;
   unsigned long long timeout_ns;
   unsigned long long* prof;  // per-CTA phase timers, or null
-  const int32_t* sbounds;    // [grid+1] SpMV block ranges, balanced by cost
 };
 
 // One problem of a solve: its operator, right-hand side, solution and the
@@ -210,6 +206,7 @@ cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cuda
 
 // Single operations (tests, residual checks).
 cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s);
+cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, cudaStream_t s);
 cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s);
 cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s);
 

@@ -6,9 +6,9 @@
 // memory is owned by its own pool allocator (the rest of the GPU is already
 // claimed), or a time-step loop that cannot afford the device-wide
 // synchronisation cudaMalloc/cudaFree can cause.  This entry point runs the
-// same FP64 persistent kernel (k_bicgstab64) with all of its scratch (seven
+// same FP64 persistent kernel (k_bicgstab64) with all of its scratch (eight
 // Krylov vectors, per-CTA reduction partials, the grid-barrier counter, the
-// abort flag, the SpMV block ranges and the statistics) in one file-scope
+// abort flag and the statistics) in one file-scope
 // static device array, so the call itself allocates nothing: no cudaMalloc,
 // no cudaFree, no allocating library routine.
 //
@@ -48,8 +48,7 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kVecBytes = align256(sizeof(double) * kNoAllocMaxCells);
 constexpr size_t kOffVec = 0;  // xo, r, rh, p, nu, t, z, z2
 constexpr size_t kOffRed = kOffVec + 8 * kVecBytes;
-constexpr size_t kOffBounds = kOffRed + align256(sizeof(double) * kRedQ * kNoAllocMaxGrid);
-constexpr size_t kOffBar = kOffBounds + align256(sizeof(int32_t) * (kNoAllocMaxGrid + 1));
+constexpr size_t kOffBar = kOffRed + align256(sizeof(double) * kRedQ * kNoAllocMaxGrid);
 constexpr size_t kOffAbort = kOffBar + 256;
 constexpr size_t kOffStats = kOffAbort + 256;
 constexpr size_t kScratchBytes = kOffStats + align256(sizeof(DevStats));
@@ -105,17 +104,7 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-  // SpMV block ranges balanced by cost (same rule as the allocating path),
-  // staged from the stack; a pageable source is copied before the call returns
-  int32_t bounds[kNoAllocMaxGrid + 1];
-  const std::vector<int32_t>& wp = *v.wprefix;
-  const int64_t W = wp.back();
-  for (int c = 0; c <= grid; ++c)
-    bounds[c] = (int32_t)(std::lower_bound(wp.begin(), wp.end(), (int32_t)(W * c / grid)) - wp.begin());
-  bounds[grid] = (int32_t)v.nb;
-  if (cudaMemcpyAsync(base + kOffBounds, bounds, sizeof(int32_t) * (grid + 1), cudaMemcpyHostToDevice, s) !=
-          cudaSuccess ||
-      cudaMemsetAsync(base + kOffBar, 0, 256, s) != cudaSuccess ||       // barrier counter starts at 0
+  if (cudaMemsetAsync(base + kOffBar, 0, 256, s) != cudaSuccess ||       // barrier counter starts at 0
       cudaMemsetAsync(base + kOffAbort, 0, 256, s) != cudaSuccess)       // abort flag starts clear
     return CUP2D_CUDA_ERROR;
 
@@ -145,7 +134,6 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   a.subtract_mean = o.subtract_mean;
   a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
   a.prof = nullptr;
-  a.sbounds = reinterpret_cast<const int32_t*>(base + kOffBounds);
 
   if (stats) cudaEventRecord(v.ev0, s);
   const cudaError_t e = launch_bicgstab64(a, grid, s);

@@ -1,15 +1,13 @@
 // Block-structured SpMV: y = A z over a range of 8x8 blocks.
 //
-// Phase 1 (stencil): one warp per block, two cells per lane; lane l owns
-// cells c0 = l (rows iy = 0..3) and c1 = l + 32 (rows 4..7).  In-block
-// neighbours come from warp shuffles; cells across a same-level face are
-// read from the neighbour block, and a wall face contributes no flux.
-// Loads of two blocks (and the epilogue's operands) are issued before either
-// is computed so that each warp keeps two blocks' worth of requests in
-// flight.  Rows of cells on a coarse/fine face are skipped here.
+// Stencil rows: the range passes (spmv_range) move 16 bytes per lane (see
+// Lane below); in-row and vertical neighbours come from warp shuffles, cells
+// across a same-level face from the neighbour block (or from another lane,
+// when that block is in the warp's span), and a wall face contributes no
+// flux.  Rows of cells on a coarse/fine face are skipped there.
 //
-// Phase 2 (explicit rows): every thread of the CTA takes explicit rows of
-// the range (they are numbered contiguously by block), one row each.
+// Explicit rows (coarse/fine faces): stored as CSR, numbered contiguously by
+// block; every thread of the CTA takes rows of the CTA's row range.
 //
 // Values written by other CTAs between grid barriers are read with
 // ld.global.cg (L2), never from a possibly stale L1 line.
@@ -30,102 +28,14 @@ __device__ __forceinline__ const double* row_vals<double>(const MeshView& M) { r
 template <>
 __device__ __forceinline__ const float* row_vals<float>(const MeshView& M) { return M.xval32; }
 
-template <class T>
-__device__ __forceinline__ T explicit_row(const MeshView& M, int r, const T* __restrict__ z) {
-  const int k0 = __ldg(M.xptr + r), k1 = __ldg(M.xptr + r + 1);
-  const T* __restrict__ vals = row_vals<T>(M);
-  T s = T(0);
-#pragma unroll 4
-  for (int k = k0; k < k1; ++k) s += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
-  return s;
-}
-
-template <class T>
-struct BlockGather {
-  int4 nb;
-  T z0, z1;                  // this lane's cells
-  T xm0, xm1, xp0, xp1;      // across the x faces (lanes with ix = 0 / 7)
-  T ym, yp;                  // across the y faces (rows 0 / 7)
-};
-
-template <class T>
-__device__ __forceinline__ void gather_block_nb(const int4& nb, int64_t blk, const T* __restrict__ z, int lane,
-                                                BlockGather<T>& g) {
-  const int ix = lane & 7, iy0 = lane >> 3;
-  g.nb = nb;
-  const int64_t o = blk * kBLEN;
-  g.z0 = ldcg(z + o + lane);
-  g.z1 = ldcg(z + o + lane + 32);
-  g.xm0 = g.xm1 = g.xp0 = g.xp1 = g.ym = g.yp = T(0);
-  if (ix == 0 && g.nb.x >= 0) {
-    const T* q = z + (int64_t)g.nb.x * kBLEN + iy0 * kBS + 7;
-    g.xm0 = ldcg(q);
-    g.xm1 = ldcg(q + 32);
-  }
-  if (ix == 7 && g.nb.y >= 0) {
-    const T* q = z + (int64_t)g.nb.y * kBLEN + iy0 * kBS;
-    g.xp0 = ldcg(q);
-    g.xp1 = ldcg(q + 32);
-  }
-  if (iy0 == 0 && g.nb.z >= 0) g.ym = ldcg(z + (int64_t)g.nb.z * kBLEN + 56 + ix);
-  if (iy0 == 3 && g.nb.w >= 0) g.yp = ldcg(z + (int64_t)g.nb.w * kBLEN + ix);
-}
-
 __device__ __forceinline__ int4 block_nbr(const MeshView& M, int64_t blk) {
   return __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
-}
-
-template <class T>
-__device__ __forceinline__ void gather_block(const MeshView& M, int64_t blk, const T* __restrict__ z, int lane,
-                                             BlockGather<T>& g) {
-  gather_block_nb<T>(block_nbr(M, blk), blk, z, lane, g);
-}
-
-// Stencil rows of the gathered block (explicit rows get meaningless values).
-template <class T>
-__device__ __forceinline__ void stencil_block(const BlockGather<T>& g, int lane, T& y0, T& y1) {
-  const int ix = lane & 7, iy0 = lane >> 3;
-  const T l0 = __shfl_up_sync(kFull, g.z0, 1), r0 = __shfl_down_sync(kFull, g.z0, 1);
-  const T l1 = __shfl_up_sync(kFull, g.z1, 1), r1 = __shfl_down_sync(kFull, g.z1, 1);
-  const T d0 = __shfl_up_sync(kFull, g.z0, 8);
-  const T u0a = __shfl_down_sync(kFull, g.z0, 8), u0b = __shfl_sync(kFull, g.z1, (lane + 8) & 31);
-  const T u1 = __shfl_down_sync(kFull, g.z1, 8);
-  const T d1a = __shfl_up_sync(kFull, g.z1, 8), d1b = __shfl_sync(kFull, g.z0, (lane + 24) & 31);
-  T a0 = T(0), a1 = T(0);
-  int n0 = 0, n1 = 0;
-  if (ix > 0) { a0 += l0; a1 += l1; n0++; n1++; }
-  else if (g.nb.x >= 0) { a0 += g.xm0; a1 += g.xm1; n0++; n1++; }
-  if (ix < 7) { a0 += r0; a1 += r1; n0++; n1++; }
-  else if (g.nb.y >= 0) { a0 += g.xp0; a1 += g.xp1; n0++; n1++; }
-  if (iy0 > 0) { a0 += d0; n0++; }
-  else if (g.nb.z >= 0) { a0 += g.ym; n0++; }
-  a0 += (lane < 24) ? u0a : u0b; n0++;
-  a1 += (lane >= 8) ? d1a : d1b; n1++;
-  if (iy0 < 3) { a1 += u1; n1++; }
-  else if (g.nb.w >= 0) { a1 += g.yp; n1++; }
-  y0 = a0 - T(n0) * g.z0;
-  y1 = a1 - T(n1) * g.z1;
 }
 
 template <class T>
 __device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, int64_t blk, const int4& nb) {
   if (nb.x == kExplicit || nb.y == kExplicit || nb.z == kExplicit || nb.w == kExplicit) return __ldg(M.xmask + blk);
   return 0ull;
-}
-
-// y = A z for the two cells of this lane (single-block form, complete rows).
-template <class T>
-__device__ __forceinline__ void spmv_block(const MeshView& M, int64_t blk, const T* __restrict__ z, int lane,
-                                           T& y0, T& y1) {
-  BlockGather<T> g;
-  gather_block<T>(M, blk, z, lane, g);
-  stencil_block<T>(g, lane, y0, y1);
-  const unsigned long long m = explicit_mask<T>(M, blk, g.nb);
-  if (m) {
-    const int base = __ldg(M.xbase + blk);
-    if ((m >> lane) & 1ull) y0 = explicit_row<T>(M, base + __popcll(m & ((1ull << lane) - 1ull)), z);
-    if ((m >> (lane + 32)) & 1ull) y1 = explicit_row<T>(M, base + __popcll(m & ((1ull << (lane + 32)) - 1ull)), z);
-  }
 }
 
 // ------------------------------------------------ 16-byte lane layout ----
@@ -200,9 +110,13 @@ struct ChunkGather {
   T ym[V], yp[V]; // across the y faces (rows 0 / 7)
 };
 
+// Loads of the lane's cells and of the halos across block faces; a face
+// whose neighbour is held by another lane of the warp (skip_*) is filled by
+// fill_siblings instead.
 template <class T>
 __device__ __forceinline__ void gather_chunk(const int4& nb, int64_t blk, bool valid, const T* __restrict__ z,
-                                             const Lane<T>& L, ChunkGather<T>& g) {
+                                             const Lane<T>& L, bool skip_xm, bool skip_xp, bool skip_ym,
+                                             bool skip_yp, ChunkGather<T>& g) {
   constexpr int V = Lane<T>::V;
   g.nb = nb;
   g.xm = g.xp = T(0);
@@ -210,10 +124,10 @@ __device__ __forceinline__ void gather_chunk(const int4& nb, int64_t blk, bool v
   for (int j = 0; j < V; ++j) g.z[j] = g.ym[j] = g.yp[j] = T(0);
   if (!valid) return;
   ldv<V>(z + blk * kBLEN + L.cell0, g.z);
-  if (L.ix0 == 0 && nb.x >= 0) g.xm = ldcg(z + (int64_t)nb.x * kBLEN + L.iy * kBS + (kBS - 1));
-  if (L.ix0 + V == kBS && nb.y >= 0) g.xp = ldcg(z + (int64_t)nb.y * kBLEN + L.iy * kBS);
-  if (L.iy == 0 && nb.z >= 0) ldv<V>(z + (int64_t)nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
-  if (L.iy == kBS - 1 && nb.w >= 0) ldv<V>(z + (int64_t)nb.w * kBLEN + L.ix0, g.yp);
+  if (L.ix0 == 0 && nb.x >= 0 && !skip_xm) g.xm = ldcg(z + (int64_t)nb.x * kBLEN + L.iy * kBS + (kBS - 1));
+  if (L.ix0 + V == kBS && nb.y >= 0 && !skip_xp) g.xp = ldcg(z + (int64_t)nb.y * kBLEN + L.iy * kBS);
+  if (L.iy == 0 && nb.z >= 0 && !skip_ym) ldv<V>(z + (int64_t)nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
+  if (L.iy == kBS - 1 && nb.w >= 0 && !skip_yp) ldv<V>(z + (int64_t)nb.w * kBLEN + L.ix0, g.yp);
 }
 
 // Stencil rows of the lane's cells, summed left, right, below, above as the
@@ -249,75 +163,156 @@ __device__ __forceinline__ void stencil_chunk(const ChunkGather<T>& g, const Lan
   }
 }
 
-// y = A z over blocks [b0, b1) by the whole CTA, in the 16-byte layout.  The
-// epilogue functor provides
+// Which faces of the lane's block in a span are shared with another block
+// of the same span (Morton siblings: the next block in x, two blocks on in
+// y for FP32 spans of four blocks).
+struct Siblings {
+  bool xm, xp, ym, yp;
+};
+
+// A warp's span: 2*CB consecutive blocks, chunk a = the first CB, chunk b =
+// the next CB.  FP32 (CB = 2): in each chunk the lower half-warp's block and
+// the upper half-warp's block are consecutive, and chunk b's blocks are two
+// on from chunk a's.  FP64 (CB = 1): chunk b's block follows chunk a's.
+template <class T>
+__device__ __forceinline__ void span_siblings(const int4& na, const int4& nbb, int64_t ba, int64_t bb, int64_t b1,
+                                              const Lane<T>& L, Siblings& sa, Siblings& sb) {
+  if constexpr (Lane<T>::CB == 2) {
+    // chunk-internal x faces (bl 0 <-> bl 1), y faces across the chunks
+    sa.xp = L.bl == 0 && na.y == ba + 1 && ba + 1 < b1;
+    sa.xm = L.bl == 1 && na.x == ba - 1;
+    sa.yp = na.w == ba + 2 && ba + 2 < b1;
+    sa.ym = false;
+    sb.xp = L.bl == 0 && nbb.y == bb + 1 && bb + 1 < b1;
+    sb.xm = L.bl == 1 && nbb.x == bb - 1;
+    sb.yp = false;
+    sb.ym = nbb.z == bb - 2 && bb < b1;
+  } else {
+    sa.xp = na.y == ba + 1 && ba + 1 < b1;
+    sa.xm = sa.ym = sa.yp = false;
+    sb.xm = nbb.x == bb - 1 && bb < b1;
+    sb.xp = sb.ym = sb.yp = false;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void fill_siblings(ChunkGather<T>& ga, ChunkGather<T>& gb, const Siblings& sa,
+                                              const Siblings& sb, const Lane<T>& L, int lane) {
+  constexpr int V = Lane<T>::V;
+  if constexpr (Lane<T>::CB == 2) {
+    // x: block bl 0's right edge <- bl 1's column 0 (lane + 15), bl 1's left
+    // edge <- bl 0's column 7 (lane - 15)
+    const T an = __shfl_sync(kFull, ga.z[0], (lane + 15) & 31), ap = __shfl_sync(kFull, ga.z[V - 1], (lane - 15) & 31);
+    const T bn = __shfl_sync(kFull, gb.z[0], (lane + 15) & 31), bp = __shfl_sync(kFull, gb.z[V - 1], (lane - 15) & 31);
+    if (sa.xp) ga.xp = an;
+    if (sa.xm) ga.xm = ap;
+    if (sb.xp) gb.xp = bn;
+    if (sb.xm) gb.xm = bp;
+    // y: chunk a's row 7 <- chunk b's row 0 (lane - 14), chunk b's row 0 <-
+    // chunk a's row 7 (lane + 14)
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const T u = __shfl_sync(kFull, gb.z[j], (lane - 14) & 31);
+      const T d = __shfl_sync(kFull, ga.z[j], (lane + 14) & 31);
+      if (sa.yp) ga.yp[j] = u;
+      if (sb.ym) gb.ym[j] = d;
+    }
+  } else {
+    // x: chunk a's right edge <- chunk b's column 0 (lane - 3), chunk b's
+    // left edge <- chunk a's column 7 (lane + 3)
+    const T n = __shfl_sync(kFull, gb.z[0], (lane - 3) & 31);
+    const T p = __shfl_sync(kFull, ga.z[V - 1], (lane + 3) & 31);
+    if (sa.xp) ga.xp = n;
+    if (sb.xm) gb.xm = p;
+  }
+  (void)L;
+}
+
+template <class T, class Epi>
+__device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGather<T>& g, const Lane<T>& L,
+                                               int64_t blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
+  constexpr int V = Lane<T>::V;
+  T y[V];
+  stencil_chunk<T>(g, L, y);
+  if (!valid) return;
+  const int64_t i0 = blk * kBLEN + L.cell0;
+  const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, g.nb) >> L.cell0) & ((1u << V) - 1u);
+  if (mk == 0u) {
+    epi.vec(i0, y, pre);
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+      if (!((mk >> j) & 1u)) epi.one(i0 + j, y[j], pre, j);
+  }
+}
+
+// y = A z: the stencil rows of blocks [b0, b1) and the explicit rows
+// [r0, r1), by the whole CTA, in the 16-byte layout.  The epilogue functor
+// provides
 //   Pre load(i0) / Pre load1(i)  operands of the lane's V cells from i0 (or
 //                                of one cell i, as element 0), loaded with
 //                                the gather, before y is known;
 //   vec(i0, y[V], pre)           the V cells (all stencil rows);
 //   one(i, y, pre, j)            cell i, element j of pre (lanes owning an
 //                                explicit row, and the explicit rows);
-// each cell is handed over exactly once, by one thread, in no particular
-// order.  A warp has two chunks in flight, and fetches the neighbour tables
-// of its next two chunks while it computes the current ones.
+// each cell of the ranges is handed over exactly once, by one thread, in no
+// particular order.  A warp takes spans of 2*CB consecutive blocks (two
+// chunks in flight), takes the halos of sibling blocks inside the span from
+// shuffles, and fetches the neighbour tables of its next span while it
+// computes the current one.  The explicit rows' offsets are fetched before
+// the stencil loop.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int64_t b0, int64_t b1,
-                                           Epi& epi) {
+                                           int64_t r0, int64_t r1, Epi& epi) {
   using Pre = typename Epi::Pre;
-  constexpr int V = Lane<T>::V, CB = Lane<T>::CB;
+  constexpr int CB = Lane<T>::CB, SPAN = 2 * CB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const Lane<T> L(lane);
-  const int64_t nch = (b1 - b0 + CB - 1) / CB;
-  auto block_of = [&](int64_t c) { return b0 + c * CB + L.bl; };
-  auto nbr_of = [&](int64_t c) {
-    const int64_t blk = block_of(c);
-    return (c < nch && blk < b1) ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
-  };
-  int64_t c = w;
-  int4 na = nbr_of(c), nbb = nbr_of(c + nw);
-  for (; c < nch; c += 2 * nw) {
-    const int64_t ca = c, cb = c + nw;
-    const int64_t ba = block_of(ca), bb = block_of(cb);
-    const bool va = ba < b1, vb = cb < nch && bb < b1;
-    ChunkGather<T> ga, gb;
-    gather_chunk<T>(na, ba, va, z, L, ga);
-    gather_chunk<T>(nbb, bb, vb, z, L, gb);
-    const int64_t ia = ba * kBLEN + L.cell0, ib = bb * kBLEN + L.cell0;
-    Pre pa{}, pb{};
-    if (va) pa = epi.load(ia);
-    if (vb) pb = epi.load(ib);
-    na = nbr_of(c + 2 * nw);
-    nbb = nbr_of(c + 3 * nw);
-    T y[V];
-    stencil_chunk<T>(ga, L, y);
-    if (va) {
-      const unsigned mk = (unsigned)(explicit_mask<T>(M, ba, ga.nb) >> L.cell0) & ((1u << V) - 1u);
-      if (mk == 0u) {
-        epi.vec(ia, y, pa);
-      } else {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-          if (!((mk >> j) & 1u)) epi.one(ia + j, y[j], pa, j);
-      }
-    }
-    stencil_chunk<T>(gb, L, y);
-    if (vb) {
-      const unsigned mk = (unsigned)(explicit_mask<T>(M, bb, gb.nb) >> L.cell0) & ((1u << V) - 1u);
-      if (mk == 0u) {
-        epi.vec(ib, y, pb);
-      } else {
-#pragma unroll
-        for (int j = 0; j < V; ++j)
-          if (!((mk >> j) & 1u)) epi.one(ib + j, y[j], pb, j);
-      }
-    }
+  // explicit rows: this thread's first row, its offsets and cell, early
+  int64_t r = r0 + threadIdx.x;
+  int k0 = 0, k1 = 0;
+  int64_t cell = 0;
+  if (r < r1) {
+    k0 = __ldg(M.xptr + r);
+    k1 = __ldg(M.xptr + r + 1);
+    cell = __ldg(M.rowcell + r);
   }
-  if (b1 > b0) {
-    const int r0 = __ldg(M.xbase + b0), r1 = __ldg(M.xbase + b1);
-    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-      const int64_t i = (int64_t)__ldg(M.rowcell + r);
-      const Pre pre = epi.load1(i);
-      epi.one(i, explicit_row<T>(M, r, z), pre, 0);
+  const int64_t nsp = (b1 - b0 + SPAN - 1) / SPAN;
+  auto nbr_of = [&](int64_t blk) {
+    return blk < b1 ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
+  };
+  int64_t sp = w;
+  int4 na = nbr_of(b0 + sp * SPAN + L.bl), nbb = nbr_of(b0 + sp * SPAN + CB + L.bl);
+  for (; sp < nsp; sp += nw) {
+    const int64_t ba = b0 + sp * SPAN + L.bl, bb = ba + CB;
+    const bool va = ba < b1, vb = bb < b1;
+    Siblings sa, sb;
+    span_siblings<T>(na, nbb, ba, bb, b1, L, sa, sb);
+    ChunkGather<T> ga, gb;
+    gather_chunk<T>(na, ba, va, z, L, sa.xm, sa.xp, sa.ym, sa.yp, ga);
+    gather_chunk<T>(nbb, bb, vb, z, L, sb.xm, sb.xp, sb.ym, sb.yp, gb);
+    Pre pa{}, pb{};
+    if (va) pa = epi.load(ba * kBLEN + L.cell0);
+    if (vb) pb = epi.load(bb * kBLEN + L.cell0);
+    const int64_t nxt = b0 + (sp + nw) * SPAN + L.bl;
+    na = nbr_of(nxt);
+    nbb = nbr_of(nxt + CB);
+    fill_siblings<T>(ga, gb, sa, sb, L, lane);
+    chunk_epilogue<T>(M, ga, L, ba, va, pa, epi);
+    chunk_epilogue<T>(M, gb, L, bb, vb, pb, epi);
+  }
+  for (; r < r1; r += blockDim.x) {
+    const Pre pre = epi.load1(cell);
+    const T* __restrict__ vals = row_vals<T>(M);
+    T acc = T(0);
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
+    epi.one(cell, acc, pre, 0);
+    const int64_t rn = r + blockDim.x;
+    if (rn < r1) {
+      k0 = __ldg(M.xptr + rn);
+      k1 = __ldg(M.xptr + rn + 1);
+      cell = __ldg(M.rowcell + rn);
     }
   }
 }

@@ -148,11 +148,12 @@ class Solver:
 
     # ------------------------------------------------------ components ---
     def apply(self, x, y, stream=None) -> None:
+        """y = A x on device tensors: float64, or float32 (the mixed form's SpMV)."""
         _check_dev(x, self.ncells)
         _check_dev(y, self.ncells)
         s = _stream_handle(stream)
-        L.check(L.lib().cup2d_poisson_apply(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s),
-                "cup2d_poisson_apply")
+        fn = L.lib().cup2d_poisson_apply32 if str(x.dtype) == "torch.float32" else L.lib().cup2d_poisson_apply
+        L.check(fn(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s), "cup2d_poisson_apply")
 
     def precond(self, p, z, stream=None) -> None:
         fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond

@@ -148,8 +148,10 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
 int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, double* d_x,
                                        cup2d_solve_stats* stats, void* stream);
 
-/* Building blocks (device buffers), exposed for parity tests. */
+/* Building blocks (device buffers), exposed for parity tests.  The operator
+ * apply is the solver's own SpMV, in FP64 and in the FP32 of the mixed form. */
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream);
+int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream);
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
 /* FP32 P^-1 apply of the mixed form (split-TF32 tensor-core MMA). */
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);
