@@ -359,6 +359,16 @@ def run_batch(args, world, rank, local) -> dict | None:
     _barrier(world)
     with ClockSampler(local) as clk:
         ms_mx, st_mx, span_mx = timed_batch("mixed", args.team_mixed)
+    if args.headline_only:
+        # profiling runs: the headline leg alone (one batched launch per step)
+        B.close()
+        tot = _max_over_ranks(sum(ms_mx), world)
+        if rank != 0:
+            return None
+        return {"metric": METRIC, "value": world * n * args.steps / (tot * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps,
+                "note": "headline leg only (profiling run)",
+                "cell_iterations_per_step": sum(s["iterations"] * c for s, c in zip(st_mx, cells))}
     ms_b64, st_b64, _ = timed_batch("fp64", args.team_fp64)
 
     # plain FP64: one handle per problem, one persistent launch per solve
@@ -636,6 +646,8 @@ def main(argv=None) -> int:
     ap.add_argument("--plain-steps", type=int, default=3, help="batch: timed steps of the one-at-a-time FP64 leg")
     ap.add_argument("--cpu-iters", type=int, default=600, help="CPU baseline: iterations per sampled problem")
     ap.add_argument("--ref-sample", type=int, default=24, help="reference arm: sampled problems")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="batch: time the batched mixed leg only (for profilers; no comparison legs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile-iters", type=int, default=0,
                     help="profiling case: capped solves only (see profile_case)")

@@ -93,6 +93,12 @@ struct Smem {
 
 // max that propagates NaN (fmax drops it, which would let a blown-up
 // residual read as converged)
+// Start of part k of n equal parts of [0, total): 64-bit product, 32-bit
+// result (cell and block indices of one problem fit in 31 bits).
+__device__ __forceinline__ int share(long long total, unsigned k, unsigned n) {
+  return (int)(total * (long long)k / (long long)n);
+}
+
 __device__ __forceinline__ double nanmax(double a, double b) { return (a > b || a != a) ? a : b; }
 
 template <int NV>
@@ -161,7 +167,7 @@ struct Pinv<double> {
     P = s.d;
   }
   __device__ __forceinline__ static double (*rows(Smem& sm, int buf))[kPad] { return sm.tile.d[buf]; }
-  __device__ __forceinline__ void apply(const double (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
+  __device__ __forceinline__ void apply(const double (*tile)[kPad], int w, int lane, int tb, int nvalid,
                                         double* __restrict__ z) const {
     const int g = lane >> 2, t = lane & 3;
     const double* arow = P[8 * w + g];
@@ -214,7 +220,7 @@ struct Pinv<float> {
     Pl = s.f[1];
   }
   __device__ __forceinline__ static float (*rows(Smem& sm, int buf))[kPad] { return sm.tile.f[buf]; }
-  __device__ __forceinline__ void apply(const float (*tile)[kPad], int w, int lane, int64_t tb, int nvalid,
+  __device__ __forceinline__ void apply(const float (*tile)[kPad], int w, int lane, int tb, int nvalid,
                                         float* __restrict__ z) const {
     const int g = lane >> 2, t = lane & 3, m = w & 3, nt = w >> 2;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -287,22 +293,22 @@ struct EpiRhNu {
   struct Pre {
     T rh[LV];
   };
-  __device__ __forceinline__ Pre load(int64_t i0) const {
+  __device__ __forceinline__ Pre load(int i0) const {
     Pre p;
     ldv<LV>(rh + i0, p.rh);
     return p;
   }
-  __device__ __forceinline__ Pre load1(int64_t i) const {
+  __device__ __forceinline__ Pre load1(int i) const {
     Pre p{};
     p.rh[0] = __ldcg(rh + i);
     return p;
   }
-  __device__ __forceinline__ void vec(int64_t i0, const T (&y)[LV], const Pre& p) {
+  __device__ __forceinline__ void vec(int i0, const T (&y)[LV], const Pre& p) {
     stv<LV>(nu + i0, y);
 #pragma unroll
     for (int j = 0; j < LV; ++j) acc += dprod(p.rh[j], y[j]);
   }
-  __device__ __forceinline__ void one(int64_t i, T y, const Pre& p, int j) {
+  __device__ __forceinline__ void one(int i, T y, const Pre& p, int j) {
     nu[i] = y;
     acc += dprod(p.rh[j], y);
   }
@@ -318,17 +324,17 @@ struct EpiTS {
   struct Pre {
     T s[LV];
   };
-  __device__ __forceinline__ Pre load(int64_t i0) const {
+  __device__ __forceinline__ Pre load(int i0) const {
     Pre p;
     ldv<LV>(s + i0, p.s);
     return p;
   }
-  __device__ __forceinline__ Pre load1(int64_t i) const {
+  __device__ __forceinline__ Pre load1(int i) const {
     Pre p{};
     p.s[0] = __ldcg(s + i);
     return p;
   }
-  __device__ __forceinline__ void vec(int64_t i0, const T (&y)[LV], const Pre& p) {
+  __device__ __forceinline__ void vec(int i0, const T (&y)[LV], const Pre& p) {
     stv<LV>(t + i0, y);
 #pragma unroll
     for (int j = 0; j < LV; ++j) {
@@ -336,7 +342,7 @@ struct EpiTS {
       tt += dprod(y[j], y[j]);
     }
   }
-  __device__ __forceinline__ void one(int64_t i, T y, const Pre& p, int j) {
+  __device__ __forceinline__ void one(int i, T y, const Pre& p, int j) {
     t[i] = y;
     ts += dprod(y, p.s[j]);
     tt += dprod(y, y);
@@ -348,7 +354,7 @@ struct EpiTS {
 __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
                                               double mean_b, const double* __restrict__ x, float* __restrict__ r,
                                               float* __restrict__ rh, bool set_rh, double* __restrict__ red,
-                                              int64_t b0, int64_t b1, int64_t r0, int64_t r1) {
+                                              int b0, int b1, int r0, int r1) {
   struct Epi {
     const double* b;
     double mean_b;
@@ -360,14 +366,14 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       double b[2];
       float rh[2];
     };
-    __device__ __forceinline__ Pre load(int64_t i0) const {
+    __device__ __forceinline__ Pre load(int i0) const {
       Pre p;
       ldv<2>(b + i0, p.b);
       if (set_rh) p.rh[0] = p.rh[1] = 0.f;
       else ldv<2>(rh + i0, p.rh);
       return p;
     }
-    __device__ __forceinline__ Pre load1(int64_t i) const {
+    __device__ __forceinline__ Pre load1(int i) const {
       Pre p{};
       p.b[0] = __ldg(b + i);
       if (!set_rh) p.rh[0] = __ldcg(rh + i);
@@ -384,14 +390,14 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       v[4] = nanmax(v[4], fabs((double)r32));
       return r32;
     }
-    __device__ __forceinline__ void vec(int64_t i0, const double (&y)[2], const Pre& p) {
+    __device__ __forceinline__ void vec(int i0, const double (&y)[2], const Pre& p) {
       float rr[2];
       rr[0] = acc(y[0], p.b[0], p.rh[0]);
       rr[1] = acc(y[1], p.b[1], p.rh[1]);
       stv<2>(r + i0, rr);
       if (set_rh) stv<2>(rh + i0, rr);
     }
-    __device__ __forceinline__ void one(int64_t i, double y, const Pre& p, int j) {
+    __device__ __forceinline__ void one(int i, double y, const Pre& p, int j) {
       const float r32 = acc(y, p.b[j], p.rh[j]);
       r[i] = r32;
       if (set_rh) rh[i] = r32;
@@ -415,8 +421,8 @@ struct MixedCtx {  // what the reliable update needs
 // replacement.  Returns false if a barrier gave up.
 template <class T, class X, bool RU>
 __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const Pinv<T>& pin,
-                              const Vecs<T, X> V, double* __restrict__ red, int64_t b0, int64_t b1,
-                              int64_t r0, int64_t r1, double tol_abs, double tol_rel, int max_restarts,
+                              const Vecs<T, X> V, double* __restrict__ red, int b0, int b1,
+                              int r0, int r1, double tol_abs, double tol_rel, int max_restarts,
                               int max_iter, const MixedCtx& mx, IterState& st) {
   constexpr int TB = Pinv<T>::kTile;
   constexpr int LV = Lane<T>::V, CB = Lane<T>::CB;  // 16-byte lane layout
@@ -452,10 +458,10 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     // tensor-core apply of the current one, so the loads overlap the apply.
     {
       T rr[LV], pp[LV], nn[LV];
-      auto load = [&](int64_t tb) {
-        const int64_t blk = tb + w * CB + L.bl;
+      auto load = [&](int tb) {
+        const int blk = tb + w * CB + L.bl;
         if (blk < b1) {
-          const int64_t i0 = blk * kBLEN + L.cell0;
+          const int i0 = blk * kBLEN + L.cell0;
           ldv<LV>(V.r + i0, rr);
           if (!zero_pnu) {
             ldv<LV>(V.p + i0, pp);
@@ -465,13 +471,13 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
       };
       int buf = 0;
       if (b0 < b1) load(b0);
-      for (int64_t tb = b0; tb < b1; tb += TB) {
+      for (int tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
         const int j = w * CB + L.bl;
         T pv[LV];
         if (j < nvalid) {
-          const int64_t i0 = (tb + j) * kBLEN + L.cell0;
+          const int i0 = (tb + j) * kBLEN + L.cell0;
 #pragma unroll
           for (int k = 0; k < LV; ++k) pv[k] = zero_pnu ? rr[k] : rr[k] + tb_beta * (pp[k] - tb_omega * nn[k]);
           if (restart_now) stv<LV>(V.rh + i0, rr);
@@ -503,23 +509,23 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     // pass C: s = r - alpha nu (in place of r); z2 = P^-1 s
     {
       T rr[LV], nn[LV];
-      auto load = [&](int64_t tb) {
-        const int64_t blk = tb + w * CB + L.bl;
+      auto load = [&](int tb) {
+        const int blk = tb + w * CB + L.bl;
         if (blk < b1) {
-          const int64_t i0 = blk * kBLEN + L.cell0;
+          const int i0 = blk * kBLEN + L.cell0;
           ldv<LV>(V.r + i0, rr);
           ldv<LV>(V.nu + i0, nn);
         }
       };
       int buf = 0;
       if (b0 < b1) load(b0);
-      for (int64_t tb = b0; tb < b1; tb += TB) {
+      for (int tb = b0; tb < b1; tb += TB) {
         const int nvalid = (int)imin64(TB, b1 - tb);
         auto tile = Pinv<T>::rows(sm, buf);
         const int j = w * CB + L.bl;
         T sv[LV];
         if (j < nvalid) {
-          const int64_t i0 = (tb + j) * kBLEN + L.cell0;
+          const int i0 = (tb + j) * kBLEN + L.cell0;
 #pragma unroll
           for (int k = 0; k < LV; ++k) sv[k] = rr[k] - ta * nn[k];
           stv<LV>(V.r + i0, sv);
@@ -553,17 +559,17 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     {
       double v[4] = {0.0, 0.0, 0.0, 0.0};
       constexpr int U = 2;
-      const int64_t nch = (b1 - b0 + CB - 1) / CB;
-      for (int64_t c0 = w; c0 < nch; c0 += U * kWarps) {
+      const int nch = (b1 - b0 + CB - 1) / CB;
+      for (int c0 = w; c0 < nch; c0 += U * kWarps) {
         X xv[U][LV];
         T zv[U][LV], z2v[U][LV], sv[U][LV], tv[U][LV], rhv[U][LV];
         bool ok[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const int64_t c = c0 + u * kWarps, blk = b0 + c * CB + L.bl;
+          const int c = c0 + u * kWarps, blk = b0 + c * CB + L.bl;
           ok[u] = c < nch && blk < b1;
           if (ok[u]) {
-            const int64_t i0 = blk * kBLEN + L.cell0;
+            const int i0 = blk * kBLEN + L.cell0;
             ldv<LV>(V.x + i0, xv[u]);
             ldv<LV>(V.z + i0, zv[u]);
             ldv<LV>(V.z2 + i0, z2v[u]);
@@ -575,7 +581,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (ok[u]) {
-            const int64_t i0 = (b0 + (c0 + u * kWarps) * CB + L.bl) * kBLEN + L.cell0;
+            const int i0 = (b0 + (c0 + u * kWarps) * CB + L.bl) * kBLEN + L.cell0;
             if (st.best_is_x) stv<LV>(V.xo + i0, xv[u]);
             X xn[LV];
             T rn[LV];
@@ -666,11 +672,11 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
 // x -= sum(h^2 x)/sum(h^2) over the CTA's blocks (ExpAMRSolver.cpp:383-415);
 // x already holds the final iterate.
 __device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, double* __restrict__ x,
-                              double* __restrict__ red, int64_t b0, int64_t b1) {
+                              double* __restrict__ red, int b0, int b1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double v[2] = {0.0, 0.0};
-  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-    const int64_t o = blk * kBLEN;
+  for (int blk = b0 + w; blk < b1; blk += kWarps) {
+    const int o = blk * kBLEN;
     const double hb = __ldg(M.hblk + blk);
     v[0] += (__ldcg(x + o + lane) + __ldcg(x + o + lane + 32)) * (hb * hb);
     v[1] += 2.0 * (hb * hb);
@@ -679,8 +685,8 @@ __device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, doubl
   if (!B.sync(&sm.flag, 7)) return false;
   grid_reduce<2>(sm, 0u, red, Q_HX);
   const double avg = sm.gres[0] / sm.gres[1];
-  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-    const int64_t o = blk * kBLEN;
+  for (int blk = b0 + w; blk < b1; blk += kWarps) {
+    const int o = blk * kBLEN;
     x[o + lane] = __ldcg(x + o + lane) - avg;
     x[o + lane + 32] = __ldcg(x + o + lane + 32) - avg;
   }
@@ -689,11 +695,11 @@ __device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, doubl
 
 // x <- x_opt when the last iterate was not the best
 __device__ __forceinline__ void take_best(bool best_is_x, double* __restrict__ x, const double* __restrict__ xo,
-                                          int64_t b0, int64_t b1) {
+                                          int b0, int b1) {
   if (best_is_x) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-    const int64_t o = blk * kBLEN;
+  for (int blk = b0 + w; blk < b1; blk += kWarps) {
+    const int o = blk * kBLEN;
     x[o + lane] = __ldcg(xo + o + lane);
     x[o + lane + 32] = __ldcg(xo + o + lane + 32);
   }
@@ -718,8 +724,8 @@ __device__ __forceinline__ void write_stats(const Smem& sm, DevStats* stats, con
 // (BiCGSTAB.cu:412-620) and the mean removal (ExpAMRSolver.cpp:383-415).
 // [b0,b1) is this CTA's block range, [r0,r1) its explicit rows.
 __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
-                           const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t r0,
-                           int64_t r1) {
+                           const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
+                           int r1) {
   const MeshView& M = pr.M;
   const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
@@ -732,12 +738,12 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
       struct Pre {
         double b[2];
       };
-      __device__ __forceinline__ Pre load(int64_t i0) const {
+      __device__ __forceinline__ Pre load(int i0) const {
         Pre p;
         ldv<2>(b + i0, p.b);
         return p;
       }
-      __device__ __forceinline__ Pre load1(int64_t i) const {
+      __device__ __forceinline__ Pre load1(int i) const {
         Pre p{};
         p.b[0] = __ldg(b + i);
         return p;
@@ -749,14 +755,14 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
         v[2] += rv * rv;
         return rv;
       }
-      __device__ __forceinline__ void vec(int64_t i0, const double (&y)[2], const Pre& p) {
+      __device__ __forceinline__ void vec(int i0, const double (&y)[2], const Pre& p) {
         double rr[2];
         rr[0] = acc(y[0], p.b[0]);
         rr[1] = acc(y[1], p.b[1]);
         stv<2>(r + i0, rr);
         stv<2>(rh + i0, rr);
       }
-      __device__ __forceinline__ void one(int64_t i, double y, const Pre& p, int j) {
+      __device__ __forceinline__ void one(int i, double y, const Pre& p, int j) {
         const double rv = acc(y, p.b[j]);
         r[i] = rv;
         rh[i] = rv;
@@ -790,15 +796,15 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
 
 // Mixed-precision solve of one problem by the team.
 __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, const ProblemMixed& pr,
-                            const SolveParams& sp, double* __restrict__ red, int64_t b0, int64_t b1, int64_t r0,
-                            int64_t r1) {
+                            const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
+                            int r1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // Neumann compatibility: project b to zero sum (sum b / n)
   {
     double v[1] = {0.0};
-    for (int64_t blk = b0 + w; blk < b1; blk += kWarps) {
-      const int64_t o = blk * kBLEN;
+    for (int blk = b0 + w; blk < b1; blk += kWarps) {
+      const int o = blk * kBLEN;
       v[0] += __ldg(pr.b + o + lane) + __ldg(pr.b + o + lane + 32);
     }
     cta_partials<1>(sm, v, 0u, red, Q_SUMB);
@@ -849,9 +855,8 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
 // the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(SolveArgs64 S) {
   __shared__ Smem sm;
-  const int64_t nb = S.M.nb;
-  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t r0 = S.M.R * blockIdx.x / gridDim.x, r1 = S.M.R * (blockIdx.x + 1) / gridDim.x;
+  const int b0 = share(S.M.nb, blockIdx.x, gridDim.x), b1 = share(S.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.M.R, blockIdx.x, gridDim.x), r1 = share(S.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -867,9 +872,8 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
 
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
   __shared__ Smem sm;
-  const int64_t nb = S.M.nb;
-  const int64_t b0 = nb * blockIdx.x / gridDim.x, b1 = nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t r0 = S.M.R * blockIdx.x / gridDim.x, r1 = S.M.R * (blockIdx.x + 1) / gridDim.x;
+  const int b0 = share(S.M.nb, blockIdx.x, gridDim.x), b1 = share(S.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.M.R, blockIdx.x, gridDim.x), r1 = share(S.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -923,13 +927,13 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
     bool ok;
     if constexpr (MIXED) {
       const ProblemMixed pr = A.pmx[p];
-      const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
-      const int64_t r0 = pr.M.R * rank / team, r1 = pr.M.R * (rank + 1) / team;
+      const int b0 = share(pr.M.nb, rank, team), b1 = share(pr.M.nb, rank + 1, team);
+      const int r0 = share(pr.M.R, rank, team), r1 = share(pr.M.R, rank + 1, team);
       ok = solve_mixed(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     } else {
       const Problem64 pr = A.p64[p];
-      const int64_t b0 = pr.M.nb * rank / team, b1 = pr.M.nb * (rank + 1) / team;
-      const int64_t r0 = pr.M.R * rank / team, r1 = pr.M.R * (rank + 1) / team;
+      const int b0 = share(pr.M.nb, rank, team), b1 = share(pr.M.nb, rank + 1, team);
+      const int r0 = share(pr.M.R, rank, team), r1 = share(pr.M.R, rank + 1, team);
       ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     }
     if (!ok) return;
@@ -992,16 +996,16 @@ struct EpiY {
   static constexpr int LV = Lane<T>::V;
   T* y;
   struct Pre {};
-  __device__ __forceinline__ Pre load(int64_t) const { return Pre{}; }
-  __device__ __forceinline__ Pre load1(int64_t) const { return Pre{}; }
-  __device__ __forceinline__ void vec(int64_t i0, const T (&v)[LV], const Pre&) { stv<LV>(y + i0, v); }
-  __device__ __forceinline__ void one(int64_t i, T v, const Pre&, int) { y[i] = v; }
+  __device__ __forceinline__ Pre load(int) const { return Pre{}; }
+  __device__ __forceinline__ Pre load1(int) const { return Pre{}; }
+  __device__ __forceinline__ void vec(int i0, const T (&v)[LV], const Pre&) { stv<LV>(y + i0, v); }
+  __device__ __forceinline__ void one(int i, T v, const Pre&, int) { y[i] = v; }
 };
 
 template <class T>
 __global__ void __launch_bounds__(kSolveThreads) k_apply(MeshView M, const T* __restrict__ x, T* __restrict__ y) {
-  const int64_t b0 = M.nb * blockIdx.x / gridDim.x, b1 = M.nb * (blockIdx.x + 1) / gridDim.x;
-  const int64_t r0 = M.R * blockIdx.x / gridDim.x, r1 = M.R * (blockIdx.x + 1) / gridDim.x;
+  const int b0 = share(M.nb, blockIdx.x, gridDim.x), b1 = share(M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(M.R, blockIdx.x, gridDim.x), r1 = share(M.R, blockIdx.x + 1, gridDim.x);
   EpiY<T> epi{y};
   spmv_range<T>(M, x, b0, b1, r0, r1, epi);
 }
@@ -1009,7 +1013,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_apply(MeshView M, const T* __
 template <class T>
 cudaError_t launch_apply(const MeshView& M, const T* x, T* y, cudaStream_t s) {
   if (M.nb <= 0) return cudaSuccess;
-  const int64_t ctas = (M.nb + 15) / 16;
+  const int ctas = (M.nb + 15) / 16;
   k_apply<T><<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(M, x, y);
   return cudaGetLastError();
 }
@@ -1022,7 +1026,7 @@ cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, cudaStrea
   return launch_apply<float>(M, x, y, s);
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int64_t nb,
+__global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int nb,
                                                              const double* __restrict__ p, double* __restrict__ z) {
   __shared__ double tile[8][kPad];
   __shared__ PinvSmem Ps;
@@ -1030,7 +1034,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __res
   Pinv<double> pin;
   pin.load(Ps, P, nullptr);
   __syncthreads();
-  for (int64_t tb = (int64_t)blockIdx.x * 8; tb < nb; tb += (int64_t)gridDim.x * 8) {
+  for (int tb = (int)blockIdx.x * 8; tb < nb; tb += (int)gridDim.x * 8) {
     const int nvalid = (int)imin64(8, nb - tb);
     if (w < nvalid) {
       tile[w][lane] = p[(tb + w) * kBLEN + lane];
@@ -1047,12 +1051,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __res
 
 cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s) {
   if (nb <= 0) return cudaSuccess;
-  const int64_t ctas = (nb + 7) / 8;
+  const int ctas = (nb + 7) / 8;
   k_precond64<<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(P, nb, p, z);
   return cudaGetLastError();
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __restrict__ P32, int64_t nb,
+__global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __restrict__ P32, int nb,
                                                              const float* __restrict__ p, float* __restrict__ z) {
   __shared__ float tile[16][kPad];
   __shared__ PinvSmem Ps;
@@ -1060,7 +1064,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __rest
   Pinv<float> pin;
   pin.load(Ps, nullptr, P32);
   __syncthreads();
-  for (int64_t tb = (int64_t)blockIdx.x * 16; tb < nb; tb += (int64_t)gridDim.x * 16) {
+  for (int tb = (int)blockIdx.x * 16; tb < nb; tb += (int)gridDim.x * 16) {
     const int nvalid = (int)imin64(16, nb - tb);
     for (int j = w; j < 16; j += kWarps) {
       tile[j][lane] = j < nvalid ? p[(tb + j) * kBLEN + lane] : 0.f;
@@ -1074,7 +1078,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __rest
 
 cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s) {
   if (nb <= 0) return cudaSuccess;
-  const int64_t ctas = (nb + 15) / 16;
+  const int ctas = (nb + 15) / 16;
   k_precond32<<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(P32, nb, p, z);
   return cudaGetLastError();
 }

@@ -80,10 +80,12 @@ struct GridBarrier {
   unsigned long long* prof;
   unsigned long long last;  // thread 0: when it left the previous barrier
 
+  // Called by all threads of the CTA; only thread 0 reads or updates the
+  // fields.
   __device__ __forceinline__ bool sync(int* smem_flag, int phase = 0) {
     __syncthreads();
-    ++epoch;
     if (threadIdx.x == 0) {
+      ++epoch;
       int ok = 1;
       unsigned long long t_arrive = 0;
       if (prof) t_arrive = globaltimer_ns();

@@ -133,37 +133,26 @@ struct SolveArgsMixed {
   unsigned long long* prof;  // per-CTA phase timers, or null
 };
 
-// One problem of a solve: its operator, right-hand side, solution and the
-// Krylov vectors it uses.
-struct Problem64 {
+// One problem of a solve: its operator, right-hand side, FP64 solution and
+// best iterate, and the Krylov vectors (type T: FP64, or FP32 for the mixed
+// form) it uses.
+template <class T>
+struct Problem {
   MeshView M;
   const double* b;
   double* x;
   double* xo;
-  double* r;
-  double* rh;
-  double* p;
-  double* nu;
-  double* t;
-  double* z;
-  double* z2;
+  T* r;   // residual; s in place between passes C and E
+  T* rh;
+  T* p;
+  T* nu;
+  T* t;
+  T* z;   // P^-1 p
+  T* z2;  // P^-1 s
   DevStats* stats;
 };
-
-struct ProblemMixed {
-  MeshView M;
-  const double* b;
-  double* x;
-  double* xo;
-  float* r;
-  float* rh;
-  float* p;
-  float* nu;
-  float* t;
-  float* z;
-  float* z2;
-  DevStats* stats;
-};
+using Problem64 = Problem<double>;
+using ProblemMixed = Problem<float>;
 
 struct SolveParams {
   double tol_abs, tol_rel, reliable_delta;

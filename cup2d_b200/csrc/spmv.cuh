@@ -28,12 +28,12 @@ __device__ __forceinline__ const double* row_vals<double>(const MeshView& M) { r
 template <>
 __device__ __forceinline__ const float* row_vals<float>(const MeshView& M) { return M.xval32; }
 
-__device__ __forceinline__ int4 block_nbr(const MeshView& M, int64_t blk) {
+__device__ __forceinline__ int4 block_nbr(const MeshView& M, int blk) {
   return __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
 }
 
 template <class T>
-__device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, int64_t blk, const int4& nb) {
+__device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, int blk, const int4& nb) {
   if (nb.x == kExplicit || nb.y == kExplicit || nb.z == kExplicit || nb.w == kExplicit) return __ldg(M.xmask + blk);
   return 0ull;
 }
@@ -114,7 +114,7 @@ struct ChunkGather {
 // whose neighbour is held by another lane of the warp (skip_*) is filled by
 // fill_siblings instead.
 template <class T>
-__device__ __forceinline__ void gather_chunk(const int4& nb, int64_t blk, bool valid, const T* __restrict__ z,
+__device__ __forceinline__ void gather_chunk(const int4& nb, int blk, bool valid, const T* __restrict__ z,
                                              const Lane<T>& L, bool skip_xm, bool skip_xp, bool skip_ym,
                                              bool skip_yp, ChunkGather<T>& g) {
   constexpr int V = Lane<T>::V;
@@ -124,10 +124,10 @@ __device__ __forceinline__ void gather_chunk(const int4& nb, int64_t blk, bool v
   for (int j = 0; j < V; ++j) g.z[j] = g.ym[j] = g.yp[j] = T(0);
   if (!valid) return;
   ldv<V>(z + blk * kBLEN + L.cell0, g.z);
-  if (L.ix0 == 0 && nb.x >= 0 && !skip_xm) g.xm = ldcg(z + (int64_t)nb.x * kBLEN + L.iy * kBS + (kBS - 1));
-  if (L.ix0 + V == kBS && nb.y >= 0 && !skip_xp) g.xp = ldcg(z + (int64_t)nb.y * kBLEN + L.iy * kBS);
-  if (L.iy == 0 && nb.z >= 0 && !skip_ym) ldv<V>(z + (int64_t)nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
-  if (L.iy == kBS - 1 && nb.w >= 0 && !skip_yp) ldv<V>(z + (int64_t)nb.w * kBLEN + L.ix0, g.yp);
+  if (L.ix0 == 0 && nb.x >= 0 && !skip_xm) g.xm = ldcg(z + nb.x * kBLEN + L.iy * kBS + (kBS - 1));
+  if (L.ix0 + V == kBS && nb.y >= 0 && !skip_xp) g.xp = ldcg(z + nb.y * kBLEN + L.iy * kBS);
+  if (L.iy == 0 && nb.z >= 0 && !skip_ym) ldv<V>(z + nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
+  if (L.iy == kBS - 1 && nb.w >= 0 && !skip_yp) ldv<V>(z + nb.w * kBLEN + L.ix0, g.yp);
 }
 
 // Stencil rows of the lane's cells, summed left, right, below, above as the
@@ -175,7 +175,7 @@ struct Siblings {
 // the upper half-warp's block are consecutive, and chunk b's blocks are two
 // on from chunk a's.  FP64 (CB = 1): chunk b's block follows chunk a's.
 template <class T>
-__device__ __forceinline__ void span_siblings(const int4& na, const int4& nbb, int64_t ba, int64_t bb, int64_t b1,
+__device__ __forceinline__ void span_siblings(const int4& na, const int4& nbb, int ba, int bb, int b1,
                                               const Lane<T>& L, Siblings& sa, Siblings& sb) {
   if constexpr (Lane<T>::CB == 2) {
     // chunk-internal x faces (bl 0 <-> bl 1), y faces across the chunks
@@ -230,12 +230,12 @@ __device__ __forceinline__ void fill_siblings(ChunkGather<T>& ga, ChunkGather<T>
 
 template <class T, class Epi>
 __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGather<T>& g, const Lane<T>& L,
-                                               int64_t blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
+                                               int blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
   constexpr int V = Lane<T>::V;
   T y[V];
   stencil_chunk<T>(g, L, y);
   if (!valid) return;
-  const int64_t i0 = blk * kBLEN + L.cell0;
+  const int i0 = blk * kBLEN + L.cell0;
   const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, g.nb) >> L.cell0) & ((1u << V) - 1u);
   if (mk == 0u) {
     epi.vec(i0, y, pre);
@@ -262,29 +262,29 @@ __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGat
 // computes the current one.  The explicit rows' offsets are fetched before
 // the stencil loop.
 template <class T, class Epi>
-__device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int64_t b0, int64_t b1,
-                                           int64_t r0, int64_t r1, Epi& epi) {
+__device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int b0, int b1,
+                                           int r0, int r1, Epi& epi) {
   using Pre = typename Epi::Pre;
   constexpr int CB = Lane<T>::CB, SPAN = 2 * CB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const Lane<T> L(lane);
   // explicit rows: this thread's first row, its offsets and cell, early
-  int64_t r = r0 + threadIdx.x;
+  int r = r0 + threadIdx.x;
   int k0 = 0, k1 = 0;
-  int64_t cell = 0;
+  int cell = 0;
   if (r < r1) {
     k0 = __ldg(M.xptr + r);
     k1 = __ldg(M.xptr + r + 1);
     cell = __ldg(M.rowcell + r);
   }
-  const int64_t nsp = (b1 - b0 + SPAN - 1) / SPAN;
-  auto nbr_of = [&](int64_t blk) {
+  const int nsp = (b1 - b0 + SPAN - 1) / SPAN;
+  auto nbr_of = [&](int blk) {
     return blk < b1 ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
   };
-  int64_t sp = w;
+  int sp = w;
   int4 na = nbr_of(b0 + sp * SPAN + L.bl), nbb = nbr_of(b0 + sp * SPAN + CB + L.bl);
   for (; sp < nsp; sp += nw) {
-    const int64_t ba = b0 + sp * SPAN + L.bl, bb = ba + CB;
+    const int ba = b0 + sp * SPAN + L.bl, bb = ba + CB;
     const bool va = ba < b1, vb = bb < b1;
     Siblings sa, sb;
     span_siblings<T>(na, nbb, ba, bb, b1, L, sa, sb);
@@ -294,7 +294,7 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
     Pre pa{}, pb{};
     if (va) pa = epi.load(ba * kBLEN + L.cell0);
     if (vb) pb = epi.load(bb * kBLEN + L.cell0);
-    const int64_t nxt = b0 + (sp + nw) * SPAN + L.bl;
+    const int nxt = b0 + (sp + nw) * SPAN + L.bl;
     na = nbr_of(nxt);
     nbb = nbr_of(nxt + CB);
     fill_siblings<T>(ga, gb, sa, sb, L, lane);
@@ -308,7 +308,7 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
 #pragma unroll 4
     for (int k = k0; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
     epi.one(cell, acc, pre, 0);
-    const int64_t rn = r + blockDim.x;
+    const int rn = r + blockDim.x;
     if (rn < r1) {
       k0 = __ldg(M.xptr + rn);
       k1 = __ldg(M.xptr + rn + 1);
