@@ -630,6 +630,21 @@ def profile_batch(args) -> int:
                 cit = sum(s["iterations"] * m.ncells for s, m in zip(st, meshes))
                 print(f"{prec} team {team}: {launch_ms:.2f} ms, {cit} cell-iterations, "
                       f"{sum(m.ncells for m in meshes)} cells", flush=True)
+        if args.phases:
+            # one full batched solve per form (rel. 1e-6) with the device phase timers on
+            for prec, team in (("fp64", args.team_fp64), ("mixed", args.team_mixed)):
+                B.set_opts(tol_rel=TOL, max_iter=20000, precision=prec, timeout_ms=120000)
+                B.set_team(team)
+                B.set_profiling(True)
+                xs = [torch.zeros_like(b) for b in bs]
+                st = B.solve_device(bs, xs)
+                _, _, launch_ms = B.timeline()
+                prof = B.profile()
+                B.set_profiling(False)
+                cit = sum(s["iterations"] * m.ncells for s, m in zip(st, meshes))
+                print(f"{prec} team {team}: launch {launch_ms:.1f} ms, {cit} cell-iterations; per CTA:", flush=True)
+                for name, (c, w) in prof.items():
+                    print(f"  {name:22s} compute {c:8.2f} ms   barrier wait {w:8.2f} ms", flush=True)
     return 0
 
 

@@ -7,7 +7,7 @@ this directory by `python -m cup2d_b200.build`.
 """
 from ._lib import Cup2dError, lib  # noqa: F401
 from .mesh import Mesh, fourier_advance, fourier_coefs  # noqa: F401
-from .poisson import (BatchSolver, ExpAMRSolver, PoissonSolver, ScalarGrid, SimulationData, Solver,  # noqa: F401
+from .poisson import (BatchSolver, ExpAMRSolver, PoissonSolver, ScalarGrid, Server, SimulationData, Solver,  # noqa: F401
                       device_pinv, make_opts, makePoissonSolver)
 
 __version__ = "0.1.0"

@@ -33,6 +33,15 @@ class SolveOpts(C.Structure):
                 ("reliable_delta", C.c_double), ("timeout_ms", C.c_int32), ("reliable_restart", C.c_int32)]
 
 
+class ServerCounters(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "failed", "queued", "inflight",
+                                        "resident_meshes", "evictions", "assemblies", "resident_bytes",
+                                        "budget_bytes")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class SolveStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
                 ("refinements", C.c_int32), ("err_init", C.c_double), ("err_final", C.c_double),
@@ -40,6 +49,11 @@ class SolveStats(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("max_inflight", C.c_int32), ("team", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("solve", SolveOpts)]
 
 
 # name -> (restype, argtypes)
@@ -80,6 +94,14 @@ SIGNATURES = {
     "cup2d_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "cup2d_batch_profile": (C.c_int, [C.c_void_p, P_f64, P_f64, C.c_int32]),
     "cup2d_batch_destroy": (C.c_int, [C.c_void_p]),
+    "cup2d_server_default_opts": (None, [C.POINTER(ServerOpts)]),
+    "cup2d_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    "cup2d_server_add_mesh": (C.c_int, [C.c_void_p, C.POINTER(Forest), P_i64]),
+    "cup2d_server_submit": (C.c_int, [C.c_void_p, C.c_int64, P_f64, P_f64, C.c_int32, P_i64]),
+    "cup2d_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(SolveStats), P_f64]),
+    "cup2d_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(SolveStats), P_f64]),
+    "cup2d_server_get_counters": (C.c_int, [C.c_void_p, C.POINTER(ServerCounters)]),
+    "cup2d_server_destroy": (C.c_int, [C.c_void_p]),
     "cup2d_mesh_disks": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                    C.c_int32, P_f64, C.c_double, C.POINTER(C.c_void_p)]),
     "cup2d_mesh_uniform": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,

@@ -255,19 +255,6 @@ struct Pinv<float> {
 
 // ----------------------------------------------------- iteration core -----
 
-template <class T, class X>
-struct Vecs {
-  X* x;   // iterate
-  X* xo;  // best iterate (lazy copy)
-  T* r;   // residual; s in place between passes C and E
-  T* rh;
-  T* p;
-  T* nu;
-  T* t;
-  T* z;   // P^-1 p
-  T* z2;  // P^-1 s
-};
-
 struct IterState {
   double rho, nr, nrh;  // (rhat,r), |r|^2, |rhat|^2 of the current residual
   double err_init;      // L-inf norm the relative test divides by
@@ -419,11 +406,12 @@ struct MixedCtx {  // what the reliable update needs
 // st.rho/nr/nrh/err_init set, p = nu = 0 implied).  T is the Krylov type,
 // X the solution type; RU enables the mixed form's true-residual
 // replacement.  Returns false if a barrier gave up.
-template <class T, class X, bool RU>
-__device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const Pinv<T>& pin,
-                              const Vecs<T, X> V, double* __restrict__ red, int b0, int b1,
-                              int r0, int r1, double tol_abs, double tol_rel, int max_restarts,
-                              int max_iter, const MixedCtx& mx, IterState& st) {
+template <class T, bool RU>
+__device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, const Problem<T>& V,
+                              double* __restrict__ red, int b0, int b1, int r0, int r1, const SolveParams& sp,
+                              const MixedCtx& mx, IterState& st) {
+  using X = double;
+  const MeshView& M = V.M;
   constexpr int TB = Pinv<T>::kTile;
   constexpr int LV = Lane<T>::V, CB = Lane<T>::CB;  // 16-byte lane layout
   static_assert(TB == CB * kWarps, "one chunk of each tile per warp");
@@ -437,14 +425,14 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
   int since = 0;                 // iterations since the last true residual
   int k;
   st.status = CUP2D_NOT_CONVERGED;
-  for (k = 0; k < max_iter; ++k) {
+  for (k = 0; k < sp.max_iter; ++k) {
     // scalar step (BiCGSTAB.cu:471-509)
     const bool serious_breakdown = rho * rho < 1e-16 * nr * nrh;
     beta = (rho / (rho_prev + eps)) * (alpha / (omega + eps));
     bool restart_now = false;
-    if (serious_breakdown && max_restarts > 0) {
+    if (serious_breakdown && sp.max_restarts > 0) {
       ++st.restarts;
-      if (st.restarts >= max_restarts) { st.status = CUP2D_BREAKDOWN_LIMIT; break; }
+      if (st.restarts >= sp.max_restarts) { st.status = CUP2D_BREAKDOWN_LIMIT; break; }
       restart_now = true;
       rho = nr;  // |rhat|^2 after rhat = r
       nrh = nr;
@@ -617,7 +605,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     if constexpr (RU) {
       rmax_since = fmax(rmax_since, sqrt(nr));
       ++since;
-      const bool claims = (error <= tol_abs) || (error / st.err_init <= tol_rel);
+      const bool claims = (error <= sp.tol_abs) || (error / st.err_init <= sp.tol_rel);
       // refresh when the FP32 residual dropped by delta, claims convergence,
       // or a sweep stalls for kMaxSweep iterations
       if (claims || sqrt(nr) < mx.delta * rmax_since || since >= kMaxSweep) {
@@ -647,7 +635,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const MeshView& M, const
     if (error < st.err_opt) {
       st.err_opt = error;
       st.best_is_x = true;
-      if (!RU && ((error <= tol_abs) || (error / st.err_init <= tol_rel))) {
+      if (!RU && ((error <= sp.tol_abs) || (error / st.err_init <= sp.tol_rel))) {
         st.status = CUP2D_OK;
         ++k;
         break;
@@ -727,7 +715,6 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
                            const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
                            int r1) {
   const MeshView& M = pr.M;
-  const Vecs<double, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
   {
     struct Epi {
@@ -785,8 +772,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
   const MixedCtx none{};
-  if (!bicgstab_loop<double, double, false>(sm, B, M, pin, V, red, b0, b1, r0, r1, sp.tol_abs, sp.tol_rel,
-                                            sp.max_restarts, sp.max_iter, none, st))
+  if (!bicgstab_loop<double, false>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, none, st))
     return false;
   take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
   if (sp.subtract_mean && !subtract_mean(sm, B, M, pr.x, red, b0, b1)) return false;
@@ -799,7 +785,6 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
                             const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
                             int r1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const Vecs<float, double> V{pr.x, pr.xo, pr.r, pr.rh, pr.p, pr.nu, pr.t, pr.z, pr.z2};
   // Neumann compatibility: project b to zero sum (sum b / n)
   {
     double v[1] = {0.0};
@@ -836,8 +821,7 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
   const bool done0 = st.err_true <= sp.tol_abs || st.err_true == 0.0;
   if (done0) {
     st.status = CUP2D_OK;
-  } else if (!bicgstab_loop<float, double, true>(sm, B, pr.M, pin, V, red, b0, b1, r0, r1, sp.tol_abs,
-                                                 sp.tol_rel, sp.max_restarts, sp.max_iter, mx, st)) {
+  } else if (!bicgstab_loop<float, true>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, mx, st)) {
     return false;
   }
   take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
@@ -853,10 +837,10 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
 // Three CTAs per SM (80 registers): the passes are bound by per-warp memory
 // latency, and the extra warps outweigh the spills this costs (measured on
 // the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(SolveArgs64 S) {
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(const __grid_constant__ SolveArgs64 S) {
   __shared__ Smem sm;
-  const int b0 = share(S.M.nb, blockIdx.x, gridDim.x), b1 = share(S.M.nb, blockIdx.x + 1, gridDim.x);
-  const int r0 = share(S.M.R, blockIdx.x, gridDim.x), r1 = share(S.M.R, blockIdx.x + 1, gridDim.x);
+  const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -865,15 +849,13 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(S
   Pinv<double> pin;
   pin.load(sm.P, S.P, nullptr);
   __syncthreads();
-  const Problem64 pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
-  const SolveParams sp{S.tol_abs, S.tol_rel, 0.0, S.max_restarts, S.max_iter, S.subtract_mean, 0};
-  solve_fp64(sm, B, pin, pr, sp, S.red, b0, b1, r0, r1);
+  solve_fp64(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
 }
 
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(SolveArgsMixed S) {
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(const __grid_constant__ SolveArgsMixed S) {
   __shared__ Smem sm;
-  const int b0 = share(S.M.nb, blockIdx.x, gridDim.x), b1 = share(S.M.nb, blockIdx.x + 1, gridDim.x);
-  const int r0 = share(S.M.R, blockIdx.x, gridDim.x), r1 = share(S.M.R, blockIdx.x + 1, gridDim.x);
+  const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
   if (threadIdx.x == 0) {
     sm.team_rank = blockIdx.x;
@@ -882,10 +864,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   Pinv<float> pin;
   pin.load(sm.P, nullptr, S.P32);
   __syncthreads();
-  const ProblemMixed pr{S.M, S.b, S.x, S.xo, S.r, S.rh, S.p, S.nu, S.t, S.z, S.z2, S.stats};
-  const SolveParams sp{S.tol_abs, S.tol_rel, S.reliable_delta, S.max_restarts, S.max_iter, S.subtract_mean,
-                       S.reliable_restart};
-  solve_mixed(sm, B, pin, pr, sp, S.red, b0, b1, r0, r1);
+  solve_mixed(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
 }
 
 // ========================================================= batches ========
@@ -926,12 +905,12 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
     const int p = __ldg(A.order + q);
     bool ok;
     if constexpr (MIXED) {
-      const ProblemMixed pr = A.pmx[p];
+      const ProblemMixed& pr = A.pmx[p];
       const int b0 = share(pr.M.nb, rank, team), b1 = share(pr.M.nb, rank + 1, team);
       const int r0 = share(pr.M.R, rank, team), r1 = share(pr.M.R, rank + 1, team);
       ok = solve_mixed(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     } else {
-      const Problem64 pr = A.p64[p];
+      const Problem64& pr = A.p64[p];
       const int b0 = share(pr.M.nb, rank, team), b1 = share(pr.M.nb, rank + 1, team);
       const int r0 = share(pr.M.R, rank, team), r1 = share(pr.M.R, rank + 1, team);
       ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
@@ -945,11 +924,11 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch64(BatchArgs A) {
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch64(const __grid_constant__ BatchArgs A) {
   batch_body<false>(A);
 }
 
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch_mixed(BatchArgs A) {
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch_mixed(const __grid_constant__ BatchArgs A) {
   batch_body<true>(A);
 }
 

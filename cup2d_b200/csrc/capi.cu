@@ -411,55 +411,26 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
   if (o.precision == CUP2D_PREC_MIXED) {
     if ((st = ensure_mixed(h))) return st;
     SolveArgsMixed a{};
-    a.M = h->mesh.view();
+    a.prob = ProblemMixed{h->mesh.view(), d_b, d_x, h->xo.p, h->f_r.p, h->f_rh.p, h->f_p.p, h->f_nu.p,
+                          h->f_t.p, h->f_z.p, h->f_z2.p, h->dstats.p};
     a.P32 = h->P32.p;
-    a.b = d_b;
-    a.x = d_x;
-    a.xo = h->xo.p;
-    a.r = h->f_r.p;
-    a.rh = h->f_rh.p;
-    a.p = h->f_p.p;
-    a.nu = h->f_nu.p;
-    a.t = h->f_t.p;
-    a.z = h->f_z.p;
-    a.z2 = h->f_z2.p;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
-    a.stats = h->dstats.p;
-    a.tol_abs = o.tol_abs;
-    a.tol_rel = o.tol_rel;
-    a.reliable_delta = o.reliable_delta;
-    a.reliable_restart = o.reliable_restart;
-    a.max_restarts = o.max_restarts;
-    a.max_iter = o.max_iter;
-    a.subtract_mean = o.subtract_mean;
+    a.sp = SolveParams{o.tol_abs, o.tol_rel, o.reliable_delta, o.max_restarts, o.max_iter, o.subtract_mean,
+                       o.reliable_restart};
     a.timeout_ns = tns;
     a.prof = prof;
     e = launch_bicgstab_mixed(a, grid, s);
   } else {
     SolveArgs64 a{};
-    a.M = h->mesh.view();
+    a.prob = Problem64{h->mesh.view(), d_b, d_x, h->xo.p, h->r.p, h->rh.p, h->p.p, h->nu.p, h->t.p, h->z.p,
+                       h->z2.p, h->dstats.p};
     a.P = h->P.p;
-    a.b = d_b;
-    a.x = d_x;
-    a.xo = h->xo.p;
-    a.r = h->r.p;
-    a.rh = h->rh.p;
-    a.p = h->p.p;
-    a.nu = h->nu.p;
-    a.t = h->t.p;
-    a.z = h->z.p;
-    a.z2 = h->z2.p;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
-    a.stats = h->dstats.p;
-    a.tol_abs = o.tol_abs;
-    a.tol_rel = o.tol_rel;
-    a.max_restarts = o.max_restarts;
-    a.max_iter = o.max_iter;
-    a.subtract_mean = o.subtract_mean;
+    a.sp = SolveParams{o.tol_abs, o.tol_rel, 0.0, o.max_restarts, o.max_iter, o.subtract_mean, 0};
     a.timeout_ns = tns;
     a.prof = prof;
     e = launch_bicgstab64(a, grid, s);
@@ -947,6 +918,68 @@ int cup2d_batch_timeline(const cup2d_batch* B, double* begin_ms, double* end_ms,
 }  // extern "C"
 
 namespace cup2d {
+
+int64_t handle_bytes(const cup2d_poisson* h) {
+  if (!h) return 0;
+  int64_t n = 0;
+  const DevBuf<int32_t>* i32[] = {&h->level, &h->bx, &h->by, &h->table, &h->nbr, &h->xcount, &h->xbase,
+                                  &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol, &h->rowcell};
+  for (auto* b : i32) n += b->cap * (int64_t)sizeof(int32_t);
+  n += h->xmask.cap * (int64_t)sizeof(unsigned long long);
+  const DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu,
+                                 &h->t, &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
+  for (auto* b : f64) n += b->cap * (int64_t)sizeof(double);
+  const DevBuf<float>* f32[] = {&h->xval32, &h->P32, &h->f_r, &h->f_rh, &h->f_p, &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
+  for (auto* b : f32) n += b->cap * (int64_t)sizeof(float);
+  return n;
+}
+
+int handle_stage(cup2d_poisson* h, double** d_b, double** d_x) {
+  if (!h || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
+  const int64_t n = h->nb * kBLEN;
+  int st;
+  if ((st = h->bstage.ensure(n)) || (st = h->xstage.ensure(n))) return st;
+  *d_b = h->bstage.p;
+  *d_x = h->xstage.p;
+  return CUP2D_OK;
+}
+
+namespace {
+struct RawStats {
+  DevStats d;
+  int aborted;
+};
+}  // namespace
+
+size_t handle_stats_bytes() { return sizeof(RawStats); }
+
+int handle_solve_async(cup2d_poisson* h, const double* d_b, double* d_x, cudaStream_t stream, void* raw) {
+  if (!raw) return CUP2D_INVALID_ARGUMENT;
+  if (h->opts.precision == CUP2D_PREC_MIXED) {
+    const int st = ensure_mixed(h);
+    if (st) return st;
+  }
+  const int st = cup2d_poisson_solve_device(h, d_b, d_x, nullptr, stream);
+  if (st) return st;
+  auto* rs = static_cast<RawStats*>(raw);
+  if (cudaMemcpyAsync(&rs->d, h->dstats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(&rs->aborted, h->abort_flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
+}
+
+void handle_stats_from_raw(const void* raw, double solve_ms, cup2d_solve_stats* out) {
+  const auto* rs = static_cast<const RawStats*>(raw);
+  const DevStats& d = rs->d;
+  out->status = rs->aborted ? CUP2D_TIMEOUT : d.status;
+  out->iterations = d.iterations;
+  out->restarts = d.restarts;
+  out->refinements = d.refinements;
+  out->err_init = d.err_init;
+  out->err_final = d.err_opt;
+  out->rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
+  out->solve_ms = solve_ms;
+}
 
 int handle_view(const cup2d_poisson* h, HandleView* out) {
   if (!h || !out || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;

@@ -22,4 +22,18 @@ struct HandleView {
 
 int handle_view(const cup2d_poisson* h, HandleView* out);
 
+// For the request server (server.cpp).
+// Device bytes a handle holds (operator, vectors, scratch).
+int64_t handle_bytes(const cup2d_poisson* h);
+// Device copies of the right-hand side and solution owned by the handle
+// (the host-buffer solve stages through them; they persist between solves).
+int handle_stage(cup2d_poisson* h, double** d_b, double** d_x);
+// Launches the handle's solve on `stream` without waiting and queues the
+// copy of its device statistics and abort flag to the pinned `raw` (at
+// least handle_stats_bytes() bytes).
+int handle_solve_async(cup2d_poisson* h, const double* d_b, double* d_x, cudaStream_t stream, void* raw);
+size_t handle_stats_bytes();
+// Statistics from a `raw` record filled by handle_solve_async.
+void handle_stats_from_raw(const void* raw, double solve_ms, cup2d_solve_stats* out);
+
 }  // namespace cup2d

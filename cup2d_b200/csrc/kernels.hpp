@@ -86,53 +86,6 @@ struct DevStats {
 
 constexpr int kRedQ = 20;  // reduction quantities per CTA
 
-struct SolveArgs64 {
-  MeshView M;
-  const double* P;      // 64x64 row-major
-  const double* b;
-  double* x;            // x0 in, solution out
-  double* xo;           // best iterate (lazy copy)
-  double* r;            // r, and s in place
-  double* rh;
-  double* p;
-  double* nu;
-  double* t;
-  double* z;            // P^-1 p
-  double* z2;           // P^-1 s
-  double* red;          // [kRedQ][grid]
-  unsigned* bar;        // arrival counter, zeroed before launch
-  int* abort_flag;      // zeroed before launch
-  DevStats* stats;
-  double tol_abs, tol_rel;
-  int max_restarts, max_iter, subtract_mean;
-  unsigned long long timeout_ns;
-  unsigned long long* prof;  // per-CTA phase timers, or null
-};
-
-// Mixed precision: FP32 Krylov vectors, FP64 solution and true residual.
-struct SolveArgsMixed {
-  MeshView M;
-  const float* P32;     // 64x64 row-major FP32 P^-1 (rounded from the FP64 build)
-  const double* b;
-  double* x;            // FP64 solution (in/out), updated every iteration
-  double* xo;           // FP64 best iterate (lazy copy)
-  float* r;
-  float* rh;
-  float* p;
-  float* nu;
-  float* t;
-  float* z;             // P^-1 p
-  float* z2;            // P^-1 s
-  double* red;
-  unsigned* bar;
-  int* abort_flag;
-  DevStats* stats;
-  double tol_abs, tol_rel, reliable_delta;
-  int max_restarts, max_iter, subtract_mean, reliable_restart;
-  unsigned long long timeout_ns;
-  unsigned long long* prof;  // per-CTA phase timers, or null
-};
-
 // One problem of a solve: its operator, right-hand side, FP64 solution and
 // best iterate, and the Krylov vectors (type T: FP64, or FP32 for the mixed
 // form) it uses.
@@ -157,6 +110,31 @@ using ProblemMixed = Problem<float>;
 struct SolveParams {
   double tol_abs, tol_rel, reliable_delta;
   int max_restarts, max_iter, subtract_mean, reliable_restart;
+};
+
+// A single solve.  The kernels take these as __grid_constant__ parameters
+// and refer to the problem and parameters in place (no per-thread copies).
+struct SolveArgs64 {
+  Problem64 prob;       // operator, b, x (x0 in, solution out), Krylov vectors
+  const double* P;      // 64x64 row-major P^-1
+  double* red;          // [kRedQ][grid]
+  unsigned* bar;        // arrival counter, zeroed before launch
+  int* abort_flag;      // zeroed before launch
+  SolveParams sp;
+  unsigned long long timeout_ns;
+  unsigned long long* prof;  // per-CTA phase timers, or null
+};
+
+// Mixed precision: FP32 Krylov vectors, FP64 solution and true residual.
+struct SolveArgsMixed {
+  ProblemMixed prob;
+  const float* P32;     // 64x64 row-major FP32 P^-1 (rounded from the FP64 build)
+  double* red;
+  unsigned* bar;
+  int* abort_flag;
+  SolveParams sp;
+  unsigned long long timeout_ns;
+  unsigned long long* prof;  // per-CTA phase timers, or null
 };
 
 // Many problems in one launch: groups of `team` CTAs take problems from a

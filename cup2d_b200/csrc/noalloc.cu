@@ -111,27 +111,23 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   double* vec = reinterpret_cast<double*>(base + kOffVec);
   const size_t stride = kVecBytes / sizeof(double);
   SolveArgs64 a{};
-  a.M = v.M;
+  a.prob = Problem64{v.M,
+                     d_b,
+                     d_x,
+                     vec + 0 * stride,  // xo
+                     vec + 1 * stride,  // r
+                     vec + 2 * stride,  // rh
+                     vec + 3 * stride,  // p
+                     vec + 4 * stride,  // nu
+                     vec + 5 * stride,  // t
+                     vec + 6 * stride,  // z
+                     vec + 7 * stride,  // z2
+                     reinterpret_cast<DevStats*>(base + kOffStats)};
   a.P = v.P;
-  a.b = d_b;
-  a.x = d_x;
-  a.xo = vec + 0 * stride;
-  a.r = vec + 1 * stride;
-  a.rh = vec + 2 * stride;
-  a.p = vec + 3 * stride;
-  a.nu = vec + 4 * stride;
-  a.t = vec + 5 * stride;
-  a.z = vec + 6 * stride;
-  a.z2 = vec + 7 * stride;
   a.red = reinterpret_cast<double*>(base + kOffRed);
   a.bar = reinterpret_cast<unsigned*>(base + kOffBar);
   a.abort_flag = reinterpret_cast<int*>(base + kOffAbort);
-  a.stats = reinterpret_cast<DevStats*>(base + kOffStats);
-  a.tol_abs = o.tol_abs;
-  a.tol_rel = o.tol_rel;
-  a.max_restarts = o.max_restarts;
-  a.max_iter = o.max_iter;
-  a.subtract_mean = o.subtract_mean;
+  a.sp = SolveParams{o.tol_abs, o.tol_rel, 0.0, o.max_restarts, o.max_iter, o.subtract_mean, 0};
   a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
   a.prof = nullptr;
 

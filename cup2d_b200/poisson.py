@@ -299,6 +299,93 @@ class BatchSolver:
         return b, e, t.value
 
 
+class Server:
+    """Request server (no counterpart in the reference): register meshes,
+    submit solves from any thread, poll or wait for them.  Every request runs
+    as its own persistent solve of `team` CTAs; requests overlap on the
+    device as slots and memory allow.  Host arrays passed to submit must stay
+    alive (and unmodified) until the request completes; pinned memory makes
+    the copies asynchronous."""
+
+    WARM_START = 1
+
+    def __init__(self, max_inflight: int = 24, team: int = 16, hbm_budget_bytes: int = 0,
+                 opts: Optional[L.SolveOpts] = None, **kw):
+        o = L.ServerOpts()
+        L.lib().cup2d_server_default_opts(C.byref(o))
+        o.max_inflight = max_inflight
+        o.team = team
+        o.hbm_budget_bytes = hbm_budget_bytes
+        o.solve = opts if opts is not None else make_opts(**kw)
+        self._h = C.c_void_p()
+        L.check(L.lib().cup2d_server_create(C.byref(o), C.byref(self._h)), "cup2d_server_create")
+        self._keep: dict[int, tuple] = {}   # request -> (b, x) kept alive until completion
+        self._meshes: list = []
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().cup2d_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_mesh(self, mesh: Mesh) -> int:
+        f = mesh.forest()
+        mid = C.c_int64()
+        L.check(L.lib().cup2d_server_add_mesh(self._h, C.byref(f), C.byref(mid)), "cup2d_server_add_mesh")
+        self._meshes.append(mesh)
+        return mid.value
+
+    def submit(self, mesh_id: int, b: np.ndarray, x: np.ndarray, warm_start: bool = False) -> int:
+        for a in (b, x):
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("b and x must be contiguous float64 arrays")
+        rid = C.c_int64()
+        L.check(L.lib().cup2d_server_submit(self._h, int(mesh_id), _pd(b), _pd(x),
+                                            self.WARM_START if warm_start else 0, C.byref(rid)),
+                "cup2d_server_submit")
+        self._keep[rid.value] = (b, x)
+        return rid.value
+
+    def _result(self, rid: int, st: int, stats: L.SolveStats, lat: C.c_double):
+        if st == L.PENDING:
+            return None
+        self._keep.pop(rid, None)
+        d = stats.as_dict()
+        d["latency_ms"] = lat.value
+        return d
+
+    def poll(self, rid: int) -> Optional[dict]:
+        """None while the request is pending, else its statistics (once)."""
+        stats, lat = L.SolveStats(), C.c_double()
+        st = L.lib().cup2d_server_poll(self._h, int(rid), C.byref(stats), C.byref(lat))
+        if st == L.INVALID_ARGUMENT:
+            raise L.Cup2dError(st, "cup2d_server_poll")
+        return self._result(rid, st, stats, lat)
+
+    def wait(self, rid: int, timeout_ms: int = 60000) -> Optional[dict]:
+        stats, lat = L.SolveStats(), C.c_double()
+        st = L.lib().cup2d_server_wait(self._h, int(rid), int(timeout_ms), C.byref(stats), C.byref(lat))
+        if st == L.INVALID_ARGUMENT:
+            raise L.Cup2dError(st, "cup2d_server_wait")
+        return self._result(rid, st, stats, lat)
+
+    def counters(self) -> dict:
+        c = L.ServerCounters()
+        L.check(L.lib().cup2d_server_get_counters(self._h, C.byref(c)), "cup2d_server_get_counters")
+        return c.as_dict()
+
+
 def _stream_handle(stream) -> C.c_void_p:
     """cudaStream_t of a torch stream; torch's current stream by default."""
     if stream is None:

@@ -211,6 +211,49 @@ int cup2d_batch_set_profiling(cup2d_batch* B, int32_t enable);
 int cup2d_batch_profile(cup2d_batch* B, double* compute_ms, double* wait_ms, int32_t nphases);
 int cup2d_batch_destroy(cup2d_batch* B);
 
+/* ------------------------------------------------------------- serving ---- */
+/* A request server (no counterpart in the reference, which solves one
+ * simulation's step per PoissonSolver::solve call, source/Poisson/Base.h:12).
+ * Callers register meshes once and submit solves against them from any
+ * thread; a worker thread admits requests in submission order as solve slots
+ * and device memory free up, keeps each mesh's operator and vectors resident
+ * while the memory budget allows (least-recently-used idle meshes are
+ * evicted first; one request per mesh runs at a time), and runs every
+ * admitted request as its own persistent solve of `team` CTAs on a stream of
+ * its own, overlapping with the requests already running.  A request's
+ * result is bit-identical to the same solve alone (cup2d_poisson_solve with
+ * grid = team).  b is read when the request is admitted and x (x0 in,
+ * solution out) is written when it completes: both host buffers must stay
+ * valid until then (pinned memory makes the copies asynchronous). */
+typedef struct cup2d_server cup2d_server;
+typedef struct cup2d_server_opts {
+  int32_t max_inflight;      /* solves on the device at once (one stream each); default 24 */
+  int32_t team;              /* CTAs per solve; default 16 */
+  int64_t hbm_budget_bytes;  /* device memory for resident meshes; 0: 80% of the free memory */
+  cup2d_solve_opts solve;    /* tolerances and precision of every solve */
+} cup2d_server_opts;
+typedef struct cup2d_server_counters {
+  int64_t submitted, admitted, completed, failed, queued, inflight;
+  int64_t resident_meshes, evictions, assemblies;
+  int64_t resident_bytes, budget_bytes;
+} cup2d_server_counters;
+/* x0 = this mesh's last solution when it is still resident (else 0); the
+ * request's x is then only written. */
+#define CUP2D_SUBMIT_WARM_START 1
+void cup2d_server_default_opts(cup2d_server_opts* opts);
+int cup2d_server_create(const cup2d_server_opts* opts, cup2d_server** out);
+/* Copies the forest; the operator is assembled when a request first needs it. */
+int cup2d_server_add_mesh(cup2d_server* S, const cup2d_forest* forest, int64_t* mesh_id);
+int cup2d_server_submit(cup2d_server* S, int64_t mesh_id, const double* b, double* x, int32_t flags,
+                        int64_t* request_id);
+/* CUP2D_PENDING while the request runs or waits; afterwards its status, its
+ * statistics and the time from submission to completion (ms), once. */
+int cup2d_server_poll(cup2d_server* S, int64_t request_id, cup2d_solve_stats* stats, double* latency_ms);
+int cup2d_server_wait(cup2d_server* S, int64_t request_id, int32_t timeout_ms, cup2d_solve_stats* stats,
+                      double* latency_ms);
+int cup2d_server_get_counters(cup2d_server* S, cup2d_server_counters* out);
+int cup2d_server_destroy(cup2d_server* S);
+
 /* ------------------------------------------------- synthetic problems ---- */
 typedef struct cup2d_mesh cup2d_mesh;
 /* Forest refined to the finest level where a block meets the band
