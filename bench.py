@@ -469,6 +469,8 @@ def run_batch(args, world, rank, local) -> dict | None:
         "clocks": clk.summary(),
         "status_ok": all(s["status"] == 0 for s in st_mx + st_b64),
     }
+    if not args.no_serve:
+        line["serving"] = run_serve(args)
     if not args.no_cpu:
         idx = batch_sample(meshes)
         sec, tot, cores = oracle_cell_iter_seconds(meshes, seeds, idx, args.cpu_iters)
@@ -479,6 +481,94 @@ def run_batch(args, world, rank, local) -> dict | None:
                       f"range ({tot:.1f} s, OpenMP, {cores} threads): {sec * 1e9:.2f} ns per cell-iteration, scaled "
                       f"by the FP64 cell-iterations of this batch ({cit_64 / n:.3g} per solve)"}
     return line
+
+
+def run_serve(args) -> dict:
+    """Serving workload: open-loop Poisson arrivals at --serve-rate requests/s,
+    mesh sizes log-uniform in 64..20000 blocks; 30% of the requests reuse a
+    recently used (resident) mesh with a new right-hand side, the others
+    bring a mesh the server has not seen (a new mesh id: assembled on
+    admission).  Each request: x0 = 0, mixed precision to rel. 1e-6, team by
+    mesh size.  Latency = submission to completion (the server's clock)."""
+    import numpy as np
+    import torch
+
+    from cup2d_b200 import Server
+    from cup2d_b200.problems import loguniform_sizes, sized_mesh
+    rng = np.random.default_rng(7)
+    pool = [sized_mesh(rng, int(n)) for n in loguniform_sizes(rng, args.serve_pool, 64, 20000)]
+    rhs = [[torch.from_numpy(m.rhs_fourier(900 + k)).pin_memory().numpy() for k in range(3)] for m in pool]
+    # pinned solution buffers, allocated before the clock starts (a
+    # page-locked allocation serialises the device's streams)
+    free_x: dict[int, list] = {i: [torch.zeros(m.ncells, dtype=torch.float64).pin_memory().numpy()
+                                   for _ in range(args.serve_xbufs)] for i, m in enumerate(pool)}
+
+    def take_x(i):
+        if free_x[i]:
+            x = free_x[i].pop()
+            x[...] = 0.0
+            return x
+        return np.zeros(pool[i].ncells)  # pageable fallback when all are in use
+
+    n = args.serve_requests
+    gaps = rng.exponential(1.0 / args.serve_rate, size=n)
+    kinds = rng.random(n) < 0.3          # True: reuse a resident mesh
+    picks = rng.integers(len(pool), size=n)
+    S = Server(max_inflight=args.serve_inflight, team=0, blocks_per_cta=args.serve_bpc,
+               solve_share=args.serve_share, tol_rel=TOL,
+               max_iter=20000, precision="mixed", timeout_ms=120000)
+    recent: list[tuple[int, int]] = []   # (mesh id, pool index) of recently used meshes
+    busy: dict[int, tuple] = {}          # request -> (pool index, x)
+    lat, iters, statuses, solve_ms, blocks = [], [], [], [], []
+    t0 = time.perf_counter()
+    t_next = t0
+    k = 0
+    done_t = t0
+    while k < n or busy:
+        now = time.perf_counter()
+        while k < n and now >= t_next:
+            if kinds[k] and recent:
+                mid, i = recent[int(rng.integers(len(recent)))]
+            else:
+                i = int(picks[k])
+                mid = S.add_mesh(pool[i])
+                recent.append((mid, i))
+                recent[:] = recent[-16:]
+            x = take_x(i)
+            rid = S.submit(mid, rhs[i][k % 3], x)
+            busy[rid] = (i, x)
+            k += 1
+            t_next += gaps[k - 1]
+        wait_ms = 0 if k < n else 2
+        for rid in S.take_completed(timeout_ms=wait_ms):
+            st = S.poll(rid)
+            i, x = busy.pop(rid)
+            if isinstance(x, np.ndarray) and x.size == pool[i].ncells and len(free_x[i]) < args.serve_xbufs:
+                free_x[i].append(x)
+            solve_ms.append(st["solve_ms"])
+            blocks.append(pool[i].nblocks)
+            lat.append(st["latency_ms"])
+            iters.append(st["iterations"])
+            statuses.append(st["status"])
+            done_t = time.perf_counter()
+        if k < n:
+            time.sleep(max(0.0, min(0.0005, t_next - time.perf_counter())))
+    c = S.counters()
+    S.close()
+    span = done_t - t0
+    return {"metric": "served Poisson solves/s (open-loop arrivals)", "value": n / span, "unit": UNIT,
+            "offered_rate": args.serve_rate, "requests": n,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "mean": float(np.mean(lat))},
+            "iterations_mean": float(np.mean(iters)), "status_ok": all(v == 0 for v in statuses),
+            "device_busy": float(np.sum(solve_ms) / (span * 1e3)),  # mean solves running at once
+            "solve_ms": {"p50": float(np.percentile(solve_ms, 50)), "max": float(np.max(solve_ms))},
+            "blocks_mean": float(np.mean(blocks)),
+            "config": f"sizes log-uniform 64..20000 blocks (pool of {len(pool)} forests), 30% reuse a resident "
+                      f"mesh with a new RHS, 70% a new mesh id (assembled on admission); mixed, rel. 1e-6, "
+                      f"x0 = 0; {args.serve_inflight} solve slots, team = blocks/{args.serve_bpc} (2..128)",
+            "server": {k2: c[k2] for k2 in ("admitted", "completed", "failed", "assemblies", "evictions",
+                                            "resident_meshes")}}
 
 
 def cpu_baseline(mesh, b, fp64_iters: float, sample_iters: int = 60) -> dict:
@@ -654,13 +744,21 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "large", "small"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "large", "small", "serve"], default="batch")
     ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
     ap.add_argument("--team-mixed", type=int, default=16, help="batch: CTAs per problem, mixed")
     ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64")
     ap.add_argument("--plain-steps", type=int, default=3, help="batch: timed steps of the one-at-a-time FP64 leg")
     ap.add_argument("--cpu-iters", type=int, default=600, help="CPU baseline: iterations per sampled problem")
     ap.add_argument("--ref-sample", type=int, default=24, help="reference arm: sampled problems")
+    ap.add_argument("--no-serve", action="store_true", help="batch: skip the serving leg")
+    ap.add_argument("--serve-rate", type=float, default=30.0, help="serving: offered requests/s")
+    ap.add_argument("--serve-requests", type=int, default=300, help="serving: requests")
+    ap.add_argument("--serve-pool", type=int, default=40, help="serving: distinct forests")
+    ap.add_argument("--serve-inflight", type=int, default=24, help="serving: solve slots")
+    ap.add_argument("--serve-share", type=float, default=0.9, help="serving: share of solve CTAs in use")
+    ap.add_argument("--serve-bpc", type=int, default=160, help="serving: blocks per CTA of a solve's team")
+    ap.add_argument("--serve-xbufs", type=int, default=12, help="serving: pinned solution buffers per forest")
     ap.add_argument("--headline-only", action="store_true",
                     help="batch: time the batched mixed leg only (for profilers; no comparison legs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -678,7 +776,12 @@ def main(argv=None) -> int:
         line = run_reference(args, world, rank)
     else:
         world, rank, local = _dist()
-        line = (run_batch if args.workload == "batch" else run_ours)(args, world, rank, local)
+        if args.workload == "serve":
+            import torch
+            torch.cuda.set_device(local)
+            line = run_serve(args) if rank == 0 else None
+        else:
+            line = (run_batch if args.workload == "batch" else run_ours)(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

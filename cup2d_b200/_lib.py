@@ -52,8 +52,8 @@ class SolveStats(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("max_inflight", C.c_int32), ("team", C.c_int32), ("hbm_budget_bytes", C.c_int64),
-                ("solve", SolveOpts)]
+    _fields_ = [("max_inflight", C.c_int32), ("team", C.c_int32), ("blocks_per_cta", C.c_int32),
+                ("solve_share", C.c_double), ("hbm_budget_bytes", C.c_int64), ("solve", SolveOpts)]
 
 
 # name -> (restype, argtypes)
@@ -100,6 +100,7 @@ SIGNATURES = {
     "cup2d_server_submit": (C.c_int, [C.c_void_p, C.c_int64, P_f64, P_f64, C.c_int32, P_i64]),
     "cup2d_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(SolveStats), P_f64]),
     "cup2d_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(SolveStats), P_f64]),
+    "cup2d_server_take_completed": (C.c_int, [C.c_void_p, P_i64, C.c_int32, C.c_int32, P_i32]),
     "cup2d_server_get_counters": (C.c_int, [C.c_void_p, C.POINTER(ServerCounters)]),
     "cup2d_server_destroy": (C.c_int, [C.c_void_p]),
     "cup2d_mesh_disks": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,

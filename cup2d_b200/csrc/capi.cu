@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -26,17 +27,87 @@ using namespace cup2d;
 
 namespace {
 
+// Device memory comes from the stream-ordered allocator on a library
+// stream per device and host thread: unlike cudaMalloc/cudaFree this does not
+// serialise the work other streams have on the device, so handles can be
+// created and destroyed while other solves run (the request server relies
+// on it).  An allocation is complete (usable from any stream) when ensure()
+// returns; a buffer is released only when nothing uses it any more.  The
+// device's default pool keeps freed memory for reuse.
+constexpr int kMaxAllocDevices = 64;
+std::mutex g_alloc_mu;
+bool g_pool_set[kMaxAllocDevices] = {};
+thread_local cudaStream_t t_alloc_stream[kMaxAllocDevices] = {};
+
+// The calling thread's allocation stream on the current device (threads do
+// not wait for each other's allocations).
+cudaStream_t alloc_stream() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxAllocDevices) return nullptr;
+  if (!t_alloc_stream[dev]) {
+    {
+      std::lock_guard<std::mutex> g(g_alloc_mu);
+      if (!g_pool_set[dev]) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+          uint64_t keep = ~0ull;
+          cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        g_pool_set[dev] = true;
+      }
+    }
+    if (cudaStreamCreateWithFlags(&t_alloc_stream[dev], cudaStreamNonBlocking) != cudaSuccess) {
+      t_alloc_stream[dev] = nullptr;
+      return nullptr;
+    }
+  }
+  return t_alloc_stream[dev];
+}
+
+// P^-1 depends on nothing but the 8x8 block Laplacian: built once per
+// device (FP64, and rounded to FP32) and shared by every handle and batch.
+struct SharedPinv {
+  double* P = nullptr;
+  float* P32 = nullptr;
+};
+SharedPinv g_pinv[kMaxAllocDevices];
+
+int shared_pinv(const double** P, const float** P32) {
+  cudaStream_t s = alloc_stream();
+  int dev = 0;
+  if (!s || cudaGetDevice(&dev) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  std::lock_guard<std::mutex> g(g_alloc_mu);
+  SharedPinv& sp = g_pinv[dev];
+  if (!sp.P) {
+    double* p = nullptr;
+    float* p32 = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(double) * 4096, s) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&p32), sizeof(float) * 4096, s) != cudaSuccess ||
+        launch_build_pinv(p, s) != cudaSuccess || launch_convert_f64_f32(p, p32, 4096, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      cudaGetLastError();
+      return CUP2D_CUDA_ERROR;
+    }
+    sp.P = p;
+    sp.P32 = p32;
+  }
+  *P = sp.P;
+  *P32 = sp.P32;
+  return CUP2D_OK;
+}
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   int64_t cap = 0;  // elements
   int ensure(int64_t n) {
     if (n <= cap && p) return CUP2D_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
+    release();
     const int64_t m = std::max<int64_t>(n, 1);
-    if (cudaMalloc(&p, sizeof(T) * m) != cudaSuccess) {
+    cudaStream_t s = alloc_stream();
+    if (!s) return CUP2D_CUDA_ERROR;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * m, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
       cudaGetLastError();
       p = nullptr;
       return CUP2D_OOM;
@@ -45,7 +116,9 @@ struct DevBuf {
     return CUP2D_OK;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (cudaStream_t s = alloc_stream()) cudaFreeAsync(p, s);
+    }
     p = nullptr;
     cap = 0;
   }
@@ -82,8 +155,10 @@ struct cup2d_poisson {
   // operator
   DevBuf<int32_t> level, bx, by, table, nbr, xcount, xbase, scan_tmp, rowlen, xptr, xcol, rowcell;
   DevBuf<unsigned long long> xmask;
-  DevBuf<double> hblk, xval, P;
-  DevBuf<float> xval32, P32;
+  DevBuf<double> hblk, xval;
+  DevBuf<float> xval32;
+  const double* P = nullptr;  // shared per device
+  const float* P32 = nullptr;
   DevBuf<int> err;
   DeviceMesh mesh;
   // Krylov vectors (FP64)
@@ -162,11 +237,9 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
       (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
       (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
     return st;
-  // Krylov vectors
-  if ((st = h->xo.ensure(n)) || (st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) ||
-      (st = h->nu.ensure(n)) || (st = h->t.ensure(n)) || (st = h->z.ensure(n)) ||
-      (st = h->z2.ensure(n)))
-    return st;
+  // the best-iterate copy; the Krylov vectors of a precision are allocated
+  // by its first solve
+  if ((st = h->xo.ensure(n))) return st;
   cudaStream_t s = h->stream;
   if (cudaMemcpyAsync(h->level.p, f->level, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(h->bx.p, f->bx, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -210,6 +283,15 @@ int ensure_scratch(cup2d_poisson* h) {
   const int g = std::max(h->grid64, h->gridmx);
   if ((st = h->red.ensure((int64_t)kRedQ * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
       (st = h->abort_flag.ensure(1)) || (st = h->dstats.ensure(1)))
+    return st;
+  return CUP2D_OK;
+}
+
+int ensure_fp64(cup2d_poisson* h) {
+  const int64_t n = h->nb * kBLEN;
+  int st;
+  if ((st = h->r.ensure(n)) || (st = h->rh.ensure(n)) || (st = h->p.ensure(n)) || (st = h->nu.ensure(n)) ||
+      (st = h->t.ensure(n)) || (st = h->z.ensure(n)) || (st = h->z2.ensure(n)))
     return st;
   return CUP2D_OK;
 }
@@ -301,8 +383,7 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
   h->opts = o;
   cudaGetDevice(&h->device);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
-      cudaMallocHost(&h->hstats, sizeof(DevStats)) != cudaSuccess) {
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     cup2d_poisson_destroy(h);
     return CUP2D_CUDA_ERROR;
   }
@@ -313,15 +394,9 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
     return CUP2D_CUDA_ERROR;
   }
   if (const char* e = std::getenv("CUP2D_GRID")) h->grid_override = std::atoi(e);
-  if ((st = h->P.ensure(4096)) || (st = h->P32.ensure(4096)) || (st = ensure_scratch(h))) {
+  if ((st = shared_pinv(&h->P, &h->P32)) || (st = ensure_scratch(h))) {
     cup2d_poisson_destroy(h);
     return st;
-  }
-  cudaError_t e = launch_build_pinv(h->P.p, h->stream);
-  if (e == cudaSuccess) e = launch_convert_f64_f32(h->P.p, h->P32.p, 4096, h->stream);
-  if (e != cudaSuccess) {
-    cup2d_poisson_destroy(h);
-    return from_cuda(e);
   }
   if ((st = do_assemble(h, forest))) {
     cup2d_poisson_destroy(h);
@@ -333,6 +408,8 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
 
 int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest) {
   if (!h) return CUP2D_INVALID_ARGUMENT;
+  // buffers may be reallocated: let solves queued on any stream finish first
+  if (cudaDeviceSynchronize() != cudaSuccess) return CUP2D_CUDA_ERROR;
   return do_assemble(h, forest);
 }
 
@@ -354,16 +431,28 @@ int cup2d_poisson_set_grid(cup2d_poisson* h, int32_t grid) {
 
 int cup2d_poisson_destroy(cup2d_poisson* h) {
   if (!h) return CUP2D_OK;
+  // solves may have been queued on any stream: let them finish before the
+  // buffers go back to the allocator
+  cudaDeviceSynchronize();
+  return cup2d::handle_destroy_idle(h);
+}
+
+}  // extern "C"
+
+namespace cup2d {
+
+int handle_destroy_idle(cup2d_poisson* h) {
+  if (!h) return CUP2D_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   DevBuf<int32_t>* i32[] = {&h->level, &h->bx, &h->by, &h->table, &h->nbr, &h->xcount, &h->xbase,
                             &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol,
                             &h->rowcell};
   for (auto* b : i32) b->release();
   h->xmask.release();
-  DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
+  DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
                            &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
   for (auto* b : f64) b->release();
-  DevBuf<float>* f32[] = {&h->xval32, &h->P32, &h->f_r, &h->f_rh, &h->f_p,
+  DevBuf<float>* f32[] = {&h->xval32, &h->f_r, &h->f_rh, &h->f_p,
                           &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
   for (auto* b : f32) b->release();
   h->err.release();
@@ -378,6 +467,10 @@ int cup2d_poisson_destroy(cup2d_poisson* h) {
   delete h;
   return CUP2D_OK;
 }
+
+}  // namespace cup2d
+
+extern "C" {
 
 int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x, cup2d_solve_stats* stats,
                                void* stream) {
@@ -406,6 +499,12 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     }
     prof = h->prof.p;
   }
+  // the pinned statistics record is allocated when statistics are first
+  // asked for (a page-locked allocation serialises the device's streams)
+  if (stats && !h->hstats && cudaMallocHost(&h->hstats, sizeof(DevStats)) != cudaSuccess) {
+    h->hstats = nullptr;
+    return CUP2D_OOM;
+  }
   if (stats) cudaEventRecord(h->ev0, s);
   cudaError_t e;
   if (o.precision == CUP2D_PREC_MIXED) {
@@ -413,7 +512,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     SolveArgsMixed a{};
     a.prob = ProblemMixed{h->mesh.view(), d_b, d_x, h->xo.p, h->f_r.p, h->f_rh.p, h->f_p.p, h->f_nu.p,
                           h->f_t.p, h->f_z.p, h->f_z2.p, h->dstats.p};
-    a.P32 = h->P32.p;
+    a.P32 = h->P32;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
@@ -423,10 +522,11 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.prof = prof;
     e = launch_bicgstab_mixed(a, grid, s);
   } else {
+    if ((st = ensure_fp64(h))) return st;
     SolveArgs64 a{};
     a.prob = Problem64{h->mesh.view(), d_b, d_x, h->xo.p, h->r.p, h->rh.p, h->p.p, h->nu.p, h->t.p, h->z.p,
                        h->z2.p, h->dstats.p};
-    a.P = h->P.p;
+    a.P = h->P;
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
@@ -482,13 +582,13 @@ int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* 
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream) {
   if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
-  return from_cuda(launch_precond64(h->P.p, h->nb, d_p, d_z, s));
+  return from_cuda(launch_precond64(h->P, h->nb, d_p, d_z, s));
 }
 
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream) {
   if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
-  return from_cuda(launch_precond32(h->P32.p, h->nb, d_p, d_z, s));
+  return from_cuda(launch_precond32(h->P32, h->nb, d_p, d_z, s));
 }
 
 int cup2d_poisson_set_profiling(cup2d_poisson* h, int32_t enable) {
@@ -618,8 +718,8 @@ struct cup2d_batch {
   DevBuf<unsigned> bars;
   DevBuf<int> slots, queue, abort_flag;
   DevBuf<DevStats> dstats;
-  DevBuf<double> P;  // one P^-1 for all problems (it depends on nothing)
-  DevBuf<float> P32;
+  const double* P = nullptr;  // the device's shared P^-1
+  const float* P32 = nullptr;
   std::vector<Problem64> h_p64;
   std::vector<ProblemMixed> h_pmx;
   std::vector<DevStats> hstats;
@@ -637,8 +737,8 @@ extern "C" {
 
 int cup2d_batch_destroy(cup2d_batch* B) {
   if (!B) return CUP2D_OK;
-  if (B->stream) cudaStreamSynchronize(B->stream);
-  for (auto* h : B->probs) cup2d_poisson_destroy(h);
+  cudaDeviceSynchronize();  // launches may have been queued on any stream
+  for (auto* h : B->probs) cup2d::handle_destroy_idle(h);
   B->d_p64.release();
   B->d_pmx.release();
   B->d_order.release();
@@ -648,8 +748,6 @@ int cup2d_batch_destroy(cup2d_batch* B) {
   B->queue.release();
   B->abort_flag.release();
   B->dstats.release();
-  B->P.release();
-  B->P32.release();
   B->prof.release();
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
@@ -713,13 +811,11 @@ int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve
   if ((st = B->d_p64.ensure(n)) || (st = B->d_pmx.ensure(n)) || (st = B->d_order.ensure(n)) ||
       (st = B->red.ensure((int64_t)kRedQ * gmax)) || (st = B->bars.ensure(gmax)) || (st = B->slots.ensure(gmax)) ||
       (st = B->queue.ensure(1)) || (st = B->abort_flag.ensure(1)) || (st = B->dstats.ensure(n)) ||
-      (st = B->P.ensure(4096)) || (st = B->P32.ensure(4096))) {
+      (st = shared_pinv(&B->P, &B->P32))) {
     cup2d_batch_destroy(B);
     return st;
   }
-  if (launch_build_pinv(B->P.p, B->stream) != cudaSuccess ||
-      launch_convert_f64_f32(B->P.p, B->P32.p, 4096, B->stream) != cudaSuccess ||
-      cudaMemcpyAsync(B->d_order.p, B->order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, B->stream) !=
+  if (cudaMemcpyAsync(B->d_order.p, B->order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, B->stream) !=
           cudaSuccess ||
       cudaStreamSynchronize(B->stream) != cudaSuccess) {
     cup2d_batch_destroy(B);
@@ -768,7 +864,7 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
   int st;
   for (int i = 0; i < n; ++i) {
     cup2d_poisson* h = B->probs[i];
-    if (mixed && (st = ensure_mixed(h))) return st;
+    if ((st = mixed ? ensure_mixed(h) : ensure_fp64(h))) return st;
     const MeshView M = h->mesh.view();
     if (mixed)
       B->h_pmx[i] = ProblemMixed{M, d_b[i], d_x[i], h->xo.p, h->f_r.p, h->f_rh.p, h->f_p.p, h->f_nu.p,
@@ -798,8 +894,8 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
   a.order = B->d_order.p;
   a.nprob = n;
   a.team = team;
-  a.P = B->P.p;
-  a.P32 = B->P32.p;
+  a.P = B->P;
+  a.P32 = B->P32;
   a.red = B->red.p;
   a.bars = B->bars.p;
   a.slots = B->slots.p;
@@ -926,10 +1022,10 @@ int64_t handle_bytes(const cup2d_poisson* h) {
                                   &h->scan_tmp, &h->rowlen, &h->xptr, &h->xcol, &h->rowcell};
   for (auto* b : i32) n += b->cap * (int64_t)sizeof(int32_t);
   n += h->xmask.cap * (int64_t)sizeof(unsigned long long);
-  const DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->P, &h->xo, &h->r, &h->rh, &h->p, &h->nu,
+  const DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->xo, &h->r, &h->rh, &h->p, &h->nu,
                                  &h->t, &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
   for (auto* b : f64) n += b->cap * (int64_t)sizeof(double);
-  const DevBuf<float>* f32[] = {&h->xval32, &h->P32, &h->f_r, &h->f_rh, &h->f_p, &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
+  const DevBuf<float>* f32[] = {&h->xval32, &h->f_r, &h->f_rh, &h->f_p, &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
   for (auto* b : f32) n += b->cap * (int64_t)sizeof(float);
   return n;
 }
@@ -985,7 +1081,7 @@ int handle_view(const cup2d_poisson* h, HandleView* out) {
   if (!h || !out || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
   out->device = h->device;
   out->M = h->mesh.view();
-  out->P = h->P.p;
+  out->P = h->P;
   out->nb = h->nb;
   out->grid = h->grid_for(h->grid64);
   out->opts = h->opts;

@@ -33,6 +33,9 @@ int handle_stage(cup2d_poisson* h, double** d_b, double** d_x);
 // least handle_stats_bytes() bytes).
 int handle_solve_async(cup2d_poisson* h, const double* d_b, double* d_x, cudaStream_t stream, void* raw);
 size_t handle_stats_bytes();
+// Destroys a handle none of whose work is pending on any stream (the
+// public cup2d_poisson_destroy first waits for the whole device).
+int handle_destroy_idle(cup2d_poisson* h);
 // Statistics from a `raw` record filled by handle_solve_async.
 void handle_stats_from_raw(const void* raw, double solve_ms, cup2d_solve_stats* out);
 

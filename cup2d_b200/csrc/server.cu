@@ -44,8 +44,11 @@ struct Mesh {
   std::vector<int32_t> level, bx, by;
   cup2d_poisson* h = nullptr;  // resident operator and vectors, or null
   int64_t bytes = 0;           // device bytes while resident
+  int team = 0;                // CTAs of its solves
   bool busy = false;           // a request of this mesh is on the device
+  bool assembling = false;     // queued for, or in, assembly
   bool solved = false;         // the resident x holds a solution (warm starts)
+  int error = CUP2D_OK;        // assembly failed: its requests fail with this
   uint64_t last_used = 0;
 
   cup2d_forest forest() const {
@@ -76,6 +79,8 @@ struct Request {
   double* x;
   int32_t flags;
   Clock::time_point submitted, finished;
+  Clock::time_point blocked_since{};  // first time it did not fit the free CTAs
+  bool blocked = false;
   bool done = false;
   int status = CUP2D_PENDING;
   cup2d_solve_stats stats{};
@@ -86,34 +91,57 @@ struct Slot {
   cudaEvent_t t0 = nullptr, t1 = nullptr, done = nullptr;
   void* raw = nullptr;  // pinned statistics record
   int64_t request = -1; // -1: free
+  int ctas = 0;         // CTAs of the solve it runs
 };
 
 }  // namespace
 
+// Host threads work for the callers: the scheduler (run) completes and
+// admits requests; assemblers build operators for meshes that are not
+// resident, so that an assembly, whose kernels may wait for SMs held by
+// running solves, never holds up admissions.  Solves in flight are kept a
+// little below the number of solve CTAs the device holds at once
+// (cta_cap), which leaves room for assembly kernels and copies.
 struct cup2d_server {
   cup2d_server_opts opts{};
   int device = 0;
   int64_t budget = 0;
+  int cta_cap = 0, ctas_inflight = 0;
   std::vector<Slot> slots;
   std::map<int64_t, Mesh> meshes;
   std::map<int64_t, Request> requests;
   std::deque<int64_t> pending;
+  std::deque<int64_t> to_assemble;  // mesh ids
   int64_t next_mesh = 1, next_request = 1;
   uint64_t tick = 0;
   int64_t resident_bytes = 0;
   cup2d_server_counters counters{};
   std::mutex mu;
-  std::condition_variable work_cv;  // new submissions
+  std::condition_variable work_cv;  // new submissions, finished assemblies
   std::condition_variable done_cv;  // completions
+  std::condition_variable asm_cv;   // meshes to assemble
   std::thread worker;
+  std::vector<std::thread> assemblers;
+  std::deque<int64_t> completed_q;  // finished requests not yet taken
+  static constexpr int kAssemblers = 8;
   bool stop = false;
   int fatal = CUP2D_OK;  // a CUDA error that stopped the worker
 
   void run();
-  bool complete_slots();                              // mu held
-  bool admit();                                       // mu held
-  int make_resident(Mesh& m, std::unique_lock<std::mutex>& lk);
+  void run_assembler();
+  bool complete_slots();  // mu held
+  bool admit();           // mu held
+  int assemble(Mesh& m, std::unique_lock<std::mutex>& lk);
   int launch(Slot& s, int64_t rid, Request& r, Mesh& m);
+  // CTAs of a mesh's solves: opts.team, or by size when it is 0
+  int team_for(int64_t nb) const {
+    const int t = opts.team > 0
+                      ? opts.team
+                      : (int)std::min<int64_t>(128, std::max<int64_t>(2, (nb + opts.blocks_per_cta / 2) /
+                                                                                  opts.blocks_per_cta));
+    return std::min(t, cta_cap);
+  }
+  static constexpr std::chrono::milliseconds kMaxBypass{100};
 };
 
 namespace {
@@ -125,9 +153,10 @@ int server_error(cup2d_server* S, int st) {
 
 }  // namespace
 
-// Evicts idle meshes (least recently used first) until `need` more bytes fit.
-int cup2d_server::make_resident(Mesh& m, std::unique_lock<std::mutex>& lk) {
-  if (m.h) return CUP2D_OK;
+// Makes m resident: evicts idle meshes (least recently used first) until it
+// fits the budget, then assembles it with the lock released.  Returns
+// CUP2D_QUEUE_FULL when the memory is held by meshes in use.
+int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
   const int64_t need = m.estimate_bytes();
   if (need > budget) return CUP2D_OOM;
   while (resident_bytes + need > budget) {
@@ -136,37 +165,63 @@ int cup2d_server::make_resident(Mesh& m, std::unique_lock<std::mutex>& lk) {
       Mesh& c = kv.second;
       if (c.h && !c.busy && (!victim || c.last_used < victim->last_used)) victim = &c;
     }
-    if (!victim) return CUP2D_QUEUE_FULL;  // everything resident is in use: wait
-    cup2d_poisson_destroy(victim->h);
+    if (!victim) return CUP2D_QUEUE_FULL;
+    handle_destroy_idle(victim->h);  // idle: its last solve has completed
     victim->h = nullptr;
     victim->solved = false;
     resident_bytes -= victim->bytes;
     victim->bytes = 0;
     ++counters.evictions;
   }
-  // assembly runs outside the lock (it synchronises its own stream)
   const cup2d_forest f = m.forest();
   cup2d_solve_opts o = opts.solve;
+  const int team = team_for((int64_t)m.level.size());
   cup2d_poisson* h = nullptr;
   resident_bytes += need;  // reserved while assembling
   lk.unlock();
   int st = cup2d_poisson_create(&f, &o, &h);
-  if (st == CUP2D_OK) st = cup2d_poisson_set_grid(h, opts.team);
+  if (st == CUP2D_OK) st = cup2d_poisson_set_grid(h, team);
   double* db = nullptr;
   double* dx = nullptr;
   if (st == CUP2D_OK) st = handle_stage(h, &db, &dx);
   lk.lock();
   resident_bytes -= need;
   if (st != CUP2D_OK) {
-    if (h) cup2d_poisson_destroy(h);
+    if (h) handle_destroy_idle(h);
     return st;
   }
   m.h = h;
+  m.team = team;
   m.bytes = handle_bytes(h);
   resident_bytes += m.bytes;
   m.solved = false;
+  m.last_used = ++tick;
   ++counters.assemblies;
   return CUP2D_OK;
+}
+
+void cup2d_server::run_assembler() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lk(mu);
+  while (!stop) {
+    if (to_assemble.empty()) {
+      asm_cv.wait_for(lk, std::chrono::milliseconds(5));
+      continue;
+    }
+    const int64_t id = to_assemble.front();
+    to_assemble.pop_front();
+    Mesh& m = meshes.at(id);
+    const int st = assemble(m, lk);
+    if (st == CUP2D_QUEUE_FULL) {
+      // the budget is held by meshes in use: retry after a completion
+      to_assemble.push_back(id);
+      done_cv.wait_for(lk, std::chrono::milliseconds(2));
+      continue;
+    }
+    m.assembling = false;
+    if (st != CUP2D_OK) m.error = st;
+    work_cv.notify_all();
+  }
 }
 
 int cup2d_server::launch(Slot& s, int64_t rid, Request& r, Mesh& m) {
@@ -190,8 +245,6 @@ int cup2d_server::launch(Slot& s, int64_t rid, Request& r, Mesh& m) {
       cudaMemcpyAsync(r.x, dx, bytes, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
       cudaEventRecord(s.done, s.stream) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
-  s.request = rid;
-  m.last_used = ++tick;
   return CUP2D_OK;
 }
 
@@ -201,8 +254,7 @@ bool cup2d_server::complete_slots() {
     if (s.request < 0) continue;
     const cudaError_t q = cudaEventQuery(s.done);
     if (q == cudaErrorNotReady) continue;
-    auto it = requests.find(s.request);
-    Request& r = it->second;
+    Request& r = requests.at(s.request);
     Mesh& m = meshes.at(r.mesh);
     if (q != cudaSuccess) {
       r.status = CUP2D_CUDA_ERROR;
@@ -216,8 +268,11 @@ bool cup2d_server::complete_slots() {
     }
     r.finished = Clock::now();
     r.done = true;
+    completed_q.push_back(s.request);
     m.busy = false;
+    ctas_inflight -= s.ctas;
     s.request = -1;
+    s.ctas = 0;
     --counters.inflight;
     if (r.status == CUP2D_OK) ++counters.completed;
     else ++counters.failed;
@@ -226,41 +281,66 @@ bool cup2d_server::complete_slots() {
   return any;
 }
 
-// Admits pending requests in submission order while slots are free; a
-// request whose mesh is running or cannot be made resident yet stays queued
-// without blocking the ones behind it.  Called with mu held by the worker,
-// which is the only thread that removes from `pending`, changes meshes'
-// residency or touches the slots; the lock is released around assembly and
-// launches (submitters only append).
+// Admits pending requests in submission order while slots and CTAs are
+// free; a request whose mesh is running or not resident yet stays queued
+// (its mesh is handed to the assembler) without blocking the ones behind
+// it; one that does not fit the free CTAs is overtaken by smaller ones for
+// at most kMaxBypass, after which admission waits for it.  Called
+// with mu held by the scheduler, the only thread that removes from
+// `pending` or touches the slots; the lock is released around launches.
 bool cup2d_server::admit() {
   bool any = false;
   std::unique_lock<std::mutex> lk(mu, std::adopt_lock);
   const std::vector<int64_t> snapshot(pending.begin(), pending.end());
   std::vector<int64_t> leaving;
   for (const int64_t rid : snapshot) {
-    Slot* free_slot = nullptr;
-    for (Slot& s : slots)
-      if (s.request < 0) { free_slot = &s; break; }
-    if (!free_slot) break;
     Request& r = requests.at(rid);
     Mesh& m = meshes.at(r.mesh);
-    if (m.busy) continue;  // one solve per mesh at a time, in submission order
-    m.busy = true;         // claimed while it is made resident and launched
-    int st = make_resident(m, lk);
-    if (st == CUP2D_QUEUE_FULL) {  // memory frees up when running solves end
-      m.busy = false;
-      continue;
-    }
+    int st = m.error;
     if (st == CUP2D_OK) {
+      if (m.busy || m.assembling) continue;
+      if (!m.h) {
+        m.assembling = true;
+        to_assemble.push_back(r.mesh);
+        asm_cv.notify_one();
+        continue;
+      }
+      if (ctas_inflight + m.team > cta_cap) {
+        // does not fit the free CTAs: later requests that fit may go first
+        // (backfill), until this one has waited kMaxBypass; then admission
+        // stops until running solves have freed enough CTAs for it
+        const Clock::time_point now = Clock::now();
+        if (!r.blocked) {
+          r.blocked = true;
+          r.blocked_since = now;
+        }
+        if (now - r.blocked_since > kMaxBypass) break;
+        continue;
+      }
+      Slot* free_slot = nullptr;
+      for (Slot& s : slots)
+        if (s.request < 0) { free_slot = &s; break; }
+      if (!free_slot) break;
+      m.busy = true;
+      free_slot->request = rid;
+      free_slot->ctas = m.team;
+      ctas_inflight += m.team;
+      m.last_used = ++tick;
       lk.unlock();
       st = launch(*free_slot, rid, r, m);
       lk.lock();
+      if (st != CUP2D_OK) {
+        m.busy = false;
+        ctas_inflight -= free_slot->ctas;
+        free_slot->request = -1;
+        free_slot->ctas = 0;
+      }
     }
     if (st != CUP2D_OK) {
-      m.busy = false;
       r.status = st;
       r.done = true;
       r.finished = Clock::now();
+      completed_q.push_back(rid);
       ++counters.failed;
       if (st == CUP2D_CUDA_ERROR) server_error(this, st);
     } else {
@@ -273,7 +353,9 @@ bool cup2d_server::admit() {
   }
   if (!leaving.empty())
     pending.erase(std::remove_if(pending.begin(), pending.end(),
-                                 [&](int64_t id) { return std::find(leaving.begin(), leaving.end(), id) != leaving.end(); }),
+                                 [&](int64_t id) {
+                                   return std::find(leaving.begin(), leaving.end(), id) != leaving.end();
+                                 }),
                   pending.end());
   lk.release();
   return any;
@@ -285,7 +367,7 @@ void cup2d_server::run() {
   while (!stop) {
     const bool completed = complete_slots();
     const bool admitted = admit();
-    if (completed) done_cv.notify_all();
+    if (completed || admitted) done_cv.notify_all();
     if (fatal) break;
     if (completed || admitted) continue;
     if (counters.inflight > 0) {
@@ -306,6 +388,8 @@ void cup2d_server_default_opts(cup2d_server_opts* o) {
   if (!o) return;
   o->max_inflight = 24;
   o->team = 16;
+  o->blocks_per_cta = 160;
+  o->solve_share = 0.9;
   o->hbm_budget_bytes = 0;
   cup2d_default_opts(&o->solve);
 }
@@ -317,7 +401,11 @@ int cup2d_server_destroy(cup2d_server* S) {
     S->stop = true;
   }
   S->work_cv.notify_all();
+  S->asm_cv.notify_all();
+  S->done_cv.notify_all();
   if (S->worker.joinable()) S->worker.join();
+  for (std::thread& t : S->assemblers)
+    if (t.joinable()) t.join();
   cudaSetDevice(S->device);
   for (Slot& s : S->slots) {
     if (s.stream) cudaStreamSynchronize(s.stream);
@@ -328,7 +416,7 @@ int cup2d_server_destroy(cup2d_server* S) {
     if (s.stream) cudaStreamDestroy(s.stream);
   }
   for (auto& kv : S->meshes)
-    if (kv.second.h) cup2d_poisson_destroy(kv.second.h);
+    if (kv.second.h) handle_destroy_idle(kv.second.h);  // every slot stream is synchronised
   delete S;
   return CUP2D_OK;
 }
@@ -339,7 +427,8 @@ int cup2d_server_create(const cup2d_server_opts* opts, cup2d_server** out) {
   cup2d_server_opts o;
   cup2d_server_default_opts(&o);
   if (opts) o = *opts;
-  if (o.max_inflight < 1 || o.max_inflight > 256 || o.team < 1 || o.team > 1024 || o.hbm_budget_bytes < 0)
+  if (o.max_inflight < 1 || o.max_inflight > 256 || o.team < 0 || o.team > 1024 || o.blocks_per_cta < 1 ||
+      o.hbm_budget_bytes < 0 || !(o.solve_share > 0.0 && o.solve_share <= 1.0))
     return CUP2D_INVALID_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -368,7 +457,15 @@ int cup2d_server_create(const cup2d_server_opts* opts, cup2d_server** out) {
       return CUP2D_CUDA_ERROR;
     }
   }
+  const int grid_max = o.solve.precision == CUP2D_PREC_MIXED ? max_coop_grid_mixed(S->device)
+                                                              : max_coop_grid_fp64(S->device);
+  if (grid_max <= 0) {
+    cup2d_server_destroy(S);
+    return CUP2D_CUDA_ERROR;
+  }
+  S->cta_cap = std::max(1, (int)(o.solve_share * grid_max));
   S->worker = std::thread([S] { S->run(); });
+  for (int i = 0; i < cup2d_server::kAssemblers; ++i) S->assemblers.emplace_back([S] { S->run_assembler(); });
   *out = S;
   return CUP2D_OK;
 }
@@ -423,6 +520,9 @@ int finish(cup2d_server* S, std::map<int64_t, Request>::iterator it, cup2d_solve
   }
   if (latency_ms) *latency_ms = ms_between(r.submitted, r.finished);
   const int st = r.status;
+  // collected: no longer reported by take_completed
+  auto q = std::find(S->completed_q.begin(), S->completed_q.end(), it->first);
+  if (q != S->completed_q.end()) S->completed_q.erase(q);
   S->requests.erase(it);
   return st;
 }
@@ -449,6 +549,19 @@ int cup2d_server_wait(cup2d_server* S, int64_t request_id, int32_t timeout_ms, c
     if (S->done_cv.wait_until(lk, deadline) == std::cv_status::timeout && !it->second.done) return CUP2D_PENDING;
   }
   return finish(S, it, stats, latency_ms);
+}
+
+int cup2d_server_take_completed(cup2d_server* S, int64_t* ids, int32_t max_ids, int32_t timeout_ms, int32_t* n) {
+  if (!S || !ids || max_ids < 1 || timeout_ms < 0 || !n) return CUP2D_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(S->mu);
+  *n = 0;
+  if (S->completed_q.empty() && timeout_ms > 0)
+    S->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [S] { return !S->completed_q.empty() || S->fatal; });
+  while (*n < max_ids && !S->completed_q.empty()) {
+    ids[(*n)++] = S->completed_q.front();
+    S->completed_q.pop_front();
+  }
+  return S->fatal ? S->fatal : CUP2D_OK;
 }
 
 int cup2d_server_get_counters(cup2d_server* S, cup2d_server_counters* out) {

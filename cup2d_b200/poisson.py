@@ -310,11 +310,14 @@ class Server:
     WARM_START = 1
 
     def __init__(self, max_inflight: int = 24, team: int = 16, hbm_budget_bytes: int = 0,
-                 opts: Optional[L.SolveOpts] = None, **kw):
+                 opts: Optional[L.SolveOpts] = None, blocks_per_cta: int = 160, solve_share: float = 0.9,
+                 **kw):
         o = L.ServerOpts()
         L.lib().cup2d_server_default_opts(C.byref(o))
         o.max_inflight = max_inflight
         o.team = team
+        o.blocks_per_cta = blocks_per_cta
+        o.solve_share = solve_share
         o.hbm_budget_bytes = hbm_budget_bytes
         o.solve = opts if opts is not None else make_opts(**kw)
         self._h = C.c_void_p()
@@ -379,6 +382,14 @@ class Server:
         if st == L.INVALID_ARGUMENT:
             raise L.Cup2dError(st, "cup2d_server_wait")
         return self._result(rid, st, stats, lat)
+
+    def take_completed(self, max_ids: int = 256, timeout_ms: int = 0) -> list[int]:
+        """Ids of requests that finished since the last call (then poll them)."""
+        ids = (C.c_int64 * max_ids)()
+        n = C.c_int32()
+        L.check(L.lib().cup2d_server_take_completed(self._h, ids, int(max_ids), int(timeout_ms), C.byref(n)),
+                "cup2d_server_take_completed")
+        return list(ids[:n.value])
 
     def counters(self) -> dict:
         c = L.ServerCounters()

@@ -228,7 +228,12 @@ int cup2d_batch_destroy(cup2d_batch* B);
 typedef struct cup2d_server cup2d_server;
 typedef struct cup2d_server_opts {
   int32_t max_inflight;      /* solves on the device at once (one stream each); default 24 */
-  int32_t team;              /* CTAs per solve; default 16 */
+  int32_t team;              /* CTAs per solve; default 16; 0: by mesh size (one CTA per
+                                blocks_per_cta blocks, 2..128) */
+  int32_t blocks_per_cta;    /* with team 0; default 160 */
+  double solve_share;        /* share of the device's co-resident solve CTAs that solves
+                                may hold at once (the rest stays free for assembly
+                                kernels and copies); default 0.9 */
   int64_t hbm_budget_bytes;  /* device memory for resident meshes; 0: 80% of the free memory */
   cup2d_solve_opts solve;    /* tolerances and precision of every solve */
 } cup2d_server_opts;
@@ -251,6 +256,10 @@ int cup2d_server_submit(cup2d_server* S, int64_t mesh_id, const double* b, doubl
 int cup2d_server_poll(cup2d_server* S, int64_t request_id, cup2d_solve_stats* stats, double* latency_ms);
 int cup2d_server_wait(cup2d_server* S, int64_t request_id, int32_t timeout_ms, cup2d_solve_stats* stats,
                       double* latency_ms);
+/* Ids of finished requests (up to max_ids, oldest first), each reported
+ * once; waits up to timeout_ms for the first.  Then poll them for results. */
+int cup2d_server_take_completed(cup2d_server* S, int64_t* ids, int32_t max_ids, int32_t timeout_ms,
+                                int32_t* n);
 int cup2d_server_get_counters(cup2d_server* S, cup2d_server_counters* out);
 int cup2d_server_destroy(cup2d_server* S);
 

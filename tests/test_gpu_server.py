@@ -134,6 +134,27 @@ def test_server_threads(cuda):
     assert c["completed"] == 24
 
 
+def test_server_take_completed(cuda):
+    """The completion queue reports each finished request once, and no
+    request that was already collected with wait."""
+    reqs = _requests(n_per_mesh=1, seed0=700)
+    with Server(max_inflight=4, team=TEAM, tol_rel=1e-6) as S:
+        ids = [S.add_mesh(m) for m in MESHES]
+        xs = [np.zeros_like(b) for _, b in reqs]
+        rids = [S.submit(ids[i], b, x) for (i, b), x in zip(reqs, xs)]
+        first = S.wait(rids[0])
+        seen = []
+        while len(seen) < len(rids) - 1:
+            got = S.take_completed(timeout_ms=5000)
+            assert got, "no completion within 5 s"
+            seen += got
+        stats = [S.poll(r) for r in seen]
+        assert S.take_completed(timeout_ms=0) == []
+    assert first["status"] == L.OK
+    assert sorted(seen) == sorted(rids[1:])
+    assert all(s["status"] == L.OK for s in stats)
+
+
 def test_server_errors(cuda):
     m = MESHES[0]
     b = m.rhs_fourier(1)
