@@ -336,29 +336,52 @@ def run_batch(args, world, rank, local) -> dict | None:
             x.zero_()
 
     def timed_batch(precision: str, team: int):
-        """CUDA events around each batched launch on the launching stream
-        (x0 = 0 written before it); the working set is far above L2."""
+        """The launch shape is picked by the autotuner (unless --no-tune);
+        each step replays a CUDA graph of one whole batched solve (x0 = 0
+        written inside it) unless --no-graph.  CUDA events around each step
+        on the launching stream; the working set is far above L2."""
         B.set_opts(precision=precision, **opts)
         B.set_team(team)
+        B.set_occupancy(0)
+        shape = {"team": team, "ctas_per_sm": 0, "tuned": False}
+        if not args.no_tune:
+            teams = [int(t) for t in args.tune_teams.split(",")]
+            cps = [int(c) for c in args.tune_cps.split(",")]
+            zero_x()
+            t, c = B.autotune(bs, xs, teams=teams, ctas_per_sm=cps, iters=args.tune_iters)
+            shape = {"team": t, "ctas_per_sm": c, "tuned": True, "tune_iters": args.tune_iters,
+                     "rates_cell_it_per_s": {f"{k[0]}/{k[1]}": r for k, r in B.tune_rates.items()}}
+        graph = not args.no_graph
+        if graph:
+            B.capture(bs, xs, zero_x=True)
         ms = []
         for i in range(args.warmup + args.steps):
-            zero_x()
+            if not graph:
+                zero_x()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            B.solve_device(bs, xs, stream=stream, stats=False)
+            if graph:
+                B.replay(stream)
+            else:
+                B.solve_device(bs, xs, stream=stream, stats=False)
             e1.record(stream)
             torch.cuda.synchronize(dev)
             if i >= args.warmup:
                 ms.append(e0.elapsed_time(e1))
-        zero_x()
-        st = B.solve_device(bs, xs, stream=stream)
+        if graph:
+            B.replay(stream)
+            st = B.replay_stats()
+        else:
+            zero_x()
+            st = B.solve_device(bs, xs, stream=stream)
         begin, end, _ = B.timeline()
-        return ms, st, end - begin
+        shape["graph"] = graph
+        return ms, st, end - begin, shape
 
     _barrier(world)
     with ClockSampler(local) as clk:
-        ms_mx, st_mx, span_mx = timed_batch("mixed", args.team_mixed)
+        ms_mx, st_mx, span_mx, shape_mx = timed_batch("mixed", args.team_mixed)
     if args.headline_only:
         # profiling runs: the headline leg alone (one batched launch per step)
         B.close()
@@ -367,9 +390,9 @@ def run_batch(args, world, rank, local) -> dict | None:
             return None
         return {"metric": METRIC, "value": world * n * args.steps / (tot * 1e-3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps,
-                "note": "headline leg only (profiling run)",
+                "note": "headline leg only (profiling run)", "launch_shape": shape_mx,
                 "cell_iterations_per_step": sum(s["iterations"] * c for s, c in zip(st_mx, cells))}
-    ms_b64, st_b64, _ = timed_batch("fp64", args.team_fp64)
+    ms_b64, st_b64, _, shape_64 = timed_batch("fp64", args.team_fp64)
 
     # plain FP64: one handle per problem, one persistent launch per solve
     hs = [Solver(m, precision="fp64", **opts) for m in meshes]
@@ -396,7 +419,8 @@ def run_batch(args, world, rank, local) -> dict | None:
 
     # end to end through the public host-buffer API (pinned host memory)
     B.set_opts(precision="mixed", **opts)
-    B.set_team(args.team_mixed)
+    B.set_team(shape_mx["team"])
+    B.set_occupancy(shape_mx["ctas_per_sm"])
     hx = [torch.zeros(c, dtype=torch.float64).pin_memory() for c in cells]
     hbn = [b.numpy() for b in hb]
     hxn = [x.numpy() for x in hx]
@@ -441,8 +465,11 @@ def run_batch(args, world, rank, local) -> dict | None:
                                f"({min(m.nblocks for m in meshes)}..{max(m.nblocks for m in meshes)}), "
                                f"levelMax 3..6, 1-3 disks, {sum(cells)} cells in total, mesh seed {3 + 1000 * rank}",
                    "tol": "true |b-Ax|_inf / |b|_inf <= 1e-6, x0 = 0 (every problem)",
-                   "solver": f"batched mixed (FP32 Krylov, FP64 x), team {args.team_mixed} CTAs per problem",
-                   "step": f"one launch solving all {n} problems",
+                   "solver": f"batched mixed (FP32 Krylov, FP64 x), team {shape_mx['team']} CTAs per problem, "
+                             f"occupancy cap {shape_mx['ctas_per_sm'] or 'none'}",
+                   "step": f"one launch solving all {n} problems" + (", replayed from a CUDA graph"
+                                                                     if shape_mx["graph"] else ""),
+                   "launch_shape": shape_mx,
                    "l2": "inputs larger than L2 (working set ~4 GB)", "parallelism": f"replicas x{world}"},
         "latency_ms": {"step_p50": _pct(ms_mx, 0.5), "step_p99": _pct(ms_mx, 0.99),
                        "problem_span_p50": float(np.percentile(span_mx, 50)),
@@ -454,7 +481,7 @@ def run_batch(args, world, rank, local) -> dict | None:
                        "latency_ms": {"p50": _pct(lat_plain, 0.5), "p99": _pct(lat_plain, 0.99)},
                        "iterations_mean": None},
         "batched_fp64": {"value": world * n * K / (tot_b64 * 1e-3), "unit": UNIT, "ms_per_step": tot_b64 / K,
-                         "team": args.team_fp64,
+                         "launch_shape": shape_64,
                          "iterations_mean": statistics.mean(s["iterations"] for s in st_b64),
                          "roofline": {"bound": "hbm", "achieved": ach_64, "peak": peak, "unit": "GB/s",
                                       "frac": ach_64 / peak, "kernel": "k_bicgstab_batch64"}},
@@ -748,6 +775,12 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
     ap.add_argument("--team-mixed", type=int, default=16, help="batch: CTAs per problem, mixed")
     ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64")
+    ap.add_argument("--no-tune", action="store_true", help="batch: fixed teams, no autotuner")
+    ap.add_argument("--tune-iters", type=int, default=40,
+                    help="batch autotuner: iterations per problem of a candidate (0 = full solves)")
+    ap.add_argument("--tune-teams", default="8,12,16,24,32", help="batch autotuner: candidate teams")
+    ap.add_argument("--tune-cps", default="0,2", help="batch autotuner: candidate CTAs per SM (0 = all)")
+    ap.add_argument("--no-graph", action="store_true", help="batch: launch directly instead of graph replays")
     ap.add_argument("--plain-steps", type=int, default=3, help="batch: timed steps of the one-at-a-time FP64 leg")
     ap.add_argument("--cpu-iters", type=int, default=600, help="CPU baseline: iterations per sampled problem")
     ap.add_argument("--ref-sample", type=int, default=24, help="reference arm: sampled problems")

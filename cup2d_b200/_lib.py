@@ -14,6 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libcup2d_poisson.so"
 OK, NOT_CONVERGED, BREAKDOWN_LIMIT, BAD_MESH, OOM, TIMEOUT, CUDA_ERROR, INVALID_ARGUMENT, \
     NO_DEVICE, QUEUE_FULL, PENDING = range(11)
 PREC_FP64, PREC_MIXED = 0, 1
+GRAPH_ZERO_X = 1
 
 P_i32 = C.POINTER(C.c_int32)
 P_i64 = C.POINTER(C.c_int64)
@@ -89,6 +90,12 @@ SIGNATURES = {
     "cup2d_batch_num_cells": (C.c_int64, [C.c_void_p, C.c_int32]),
     "cup2d_batch_solve_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.POINTER(SolveStats), C.c_void_p]),
+    "cup2d_batch_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), P_i32, C.c_int32,
+                                   P_i32, C.c_int32, C.c_int32, P_f64, P_i32, P_i32]),
+    "cup2d_batch_set_occupancy": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cup2d_batch_capture": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32]),
+    "cup2d_batch_replay": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cup2d_batch_replay_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cup2d_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(P_f64), C.POINTER(P_f64), C.POINTER(SolveStats)]),
     "cup2d_batch_timeline": (C.c_int, [C.c_void_p, P_f64, P_f64, P_f64]),
     "cup2d_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),

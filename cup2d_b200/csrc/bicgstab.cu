@@ -960,10 +960,22 @@ int max_coop_grid_batch(int device, bool mixed) {
   return coop_grid(mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64, device);
 }
 
+// Cooperative launch through the extensible launch API, so that a stream
+// capture records the cooperative attribute in the graph's kernel node.
 cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s) {
   void* args[] = {const_cast<BatchArgs*>(&a)};
-  return cudaLaunchCooperativeKernel(mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64,
-                                     dim3(grid), dim3(kSolveThreads), args, 0, s);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kSolveThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64,
+                             args);
 }
 
 // ------------------------------------------------------- single ops -------

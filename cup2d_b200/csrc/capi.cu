@@ -703,6 +703,34 @@ int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n_out, int64_t* nnz_out,
 // of its own); the per-problem descriptors are rebuilt on the host for each
 // solve because the right-hand sides and solutions are call arguments.
 
+// One whole batched solve recorded as a CUDA graph: state resets, the
+// persistent launch, the read-back of the statistics into pinned memory.
+struct BatchGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;   // recorded after each replay
+  DevBuf<Problem64> p64;        // the graph's own problem descriptors
+  DevBuf<ProblemMixed> pmx;
+  DevStats* hstats = nullptr;   // pinned, n entries followed by the abort flag
+  int* habort = nullptr;
+  int n = 0;
+  bool replayed = false;
+  void reset() {  // the graph only; buffers stay for the next capture
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    replayed = false;
+  }
+  void release() {
+    reset();
+    p64.release();
+    pmx.release();
+    if (hstats) cudaFreeHost(hstats);
+    hstats = nullptr;
+    habort = nullptr;
+    if (done) cudaEventDestroy(done);
+    done = nullptr;
+  }
+};
+
 struct cup2d_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -711,6 +739,7 @@ struct cup2d_batch {
   std::vector<int32_t> order;  // largest first
   int team = 8;
   int grid64 = 0, gridmx = 0;
+  int sms = 0, ctas_per_sm = 0;  // occupancy cap, 0 = every co-resident CTA
   DevBuf<Problem64> d_p64;
   DevBuf<ProblemMixed> d_pmx;
   DevBuf<int32_t> d_order;
@@ -731,6 +760,7 @@ struct cup2d_batch {
   DevBuf<unsigned long long> prof;  // phase timers (profiling on)
   bool profiling = false;
   int prof_grid = 0;
+  BatchGraph graph;
 };
 
 extern "C" {
@@ -749,6 +779,7 @@ int cup2d_batch_destroy(cup2d_batch* B) {
   B->abort_flag.release();
   B->dstats.release();
   B->prof.release();
+  B->graph.release();
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->stream) cudaStreamDestroy(B->stream);
@@ -776,13 +807,15 @@ int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve
   B->opts = o;
   cudaGetDevice(&B->device);
   if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess) {
+      cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&B->graph.done, cudaEventDisableTiming) != cudaSuccess) {
     cup2d_batch_destroy(B);
     return CUP2D_CUDA_ERROR;
   }
   B->grid64 = max_coop_grid_batch(B->device, false);
   B->gridmx = max_coop_grid_batch(B->device, true);
-  if (B->grid64 <= 0 || B->gridmx <= 0) {
+  cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, B->device);
+  if (B->grid64 <= 0 || B->gridmx <= 0 || B->sms <= 0) {
     cup2d_batch_destroy(B);
     return CUP2D_CUDA_ERROR;
   }
@@ -845,6 +878,12 @@ int cup2d_batch_set_team(cup2d_batch* B, int32_t team) {
   return CUP2D_OK;
 }
 
+int cup2d_batch_set_occupancy(cup2d_batch* B, int32_t ctas_per_sm) {
+  if (!B || ctas_per_sm < 0 || ctas_per_sm > 32) return CUP2D_INVALID_ARGUMENT;
+  B->ctas_per_sm = ctas_per_sm;
+  return CUP2D_OK;
+}
+
 int32_t cup2d_batch_size(const cup2d_batch* B) { return B ? (int32_t)B->probs.size() : 0; }
 
 int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i) {
@@ -852,13 +891,20 @@ int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i) {
   return B->probs[i]->nb * kBLEN;
 }
 
-int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
-                             cup2d_solve_stats* stats, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Validates the batch's inputs, fills the host-side problem descriptors and
+// the launch arguments (descriptor arrays at the given device addresses)
+// and picks the grid: groups of `team` CTAs, as many as fit the occupancy
+// cap, never more groups than problems.
+int batch_prepare(cup2d_batch* B, const double* const* d_b, double* const* d_x, Problem64* dp64,
+                  ProblemMixed* dpmx, BatchArgs& a, int& grid) {
   if (!B || !d_b || !d_x) return CUP2D_INVALID_ARGUMENT;
   const int n = (int)B->probs.size();
   for (int i = 0; i < n; ++i)
     if (!d_b[i] || !d_x[i] || !aligned16(d_b[i]) || !aligned16(d_x[i])) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const cup2d_solve_opts& o = B->opts;
   const bool mixed = o.precision == CUP2D_PREC_MIXED;
   int st;
@@ -874,23 +920,17 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
                               B->dstats.p + i};
   }
   const int team = B->team;
-  const int gmax = mixed ? B->gridmx : B->grid64;
+  int gmax = mixed ? B->gridmx : B->grid64;
+  if (B->ctas_per_sm > 0) gmax = std::min(gmax, B->ctas_per_sm * B->sms);
   const int groups = std::max(1, std::min(gmax / team, n));
   if (groups * team > gmax) return CUP2D_INVALID_ARGUMENT;  // team larger than the device
-  const int grid = groups * team;
+  grid = groups * team;
   // per group: barriers of every problem it may take, in 32 bits
   const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)n * (uint64_t)team;
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
-  if ((mixed ? cudaMemcpyAsync(B->d_pmx.p, B->h_pmx.data(), sizeof(ProblemMixed) * n, cudaMemcpyHostToDevice, s)
-             : cudaMemcpyAsync(B->d_p64.p, B->h_p64.data(), sizeof(Problem64) * n, cudaMemcpyHostToDevice, s)) !=
-          cudaSuccess ||
-      cudaMemsetAsync(B->bars.p, 0, sizeof(unsigned) * groups, s) != cudaSuccess ||
-      cudaMemsetAsync(B->queue.p, 0, sizeof(int), s) != cudaSuccess ||
-      cudaMemsetAsync(B->abort_flag.p, 0, sizeof(int), s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  BatchArgs a{};
-  a.p64 = B->d_p64.p;
-  a.pmx = B->d_pmx.p;
+  a = BatchArgs{};
+  a.p64 = dp64;
+  a.pmx = dpmx;
   a.order = B->d_order.p;
   a.nprob = n;
   a.team = team;
@@ -905,6 +945,50 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
                      o.reliable_restart};
   a.timeout_ns = (unsigned long long)o.timeout_ms * 1000000ull;
   a.prof = nullptr;
+  return CUP2D_OK;
+}
+
+// The per-launch state resets and the launch itself, in stream order.
+cudaError_t batch_enqueue(cup2d_batch* B, const BatchArgs& a, int grid, int groups, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(B->bars.p, 0, sizeof(unsigned) * groups, s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(B->queue.p, 0, sizeof(int), s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(B->abort_flag.p, 0, sizeof(int), s)) != cudaSuccess)
+    return e;
+  return launch_bicgstab_batch(a, grid, B->opts.precision == CUP2D_PREC_MIXED, s);
+}
+
+void batch_fill_stats(const DevStats* hs, int n, int aborted, float ms, cup2d_solve_stats* stats) {
+  for (int i = 0; i < n; ++i) {
+    const DevStats& d = hs[i];
+    stats[i].status = aborted ? CUP2D_TIMEOUT : d.status;
+    stats[i].iterations = d.iterations;
+    stats[i].restarts = d.restarts;
+    stats[i].refinements = d.refinements;
+    stats[i].err_init = d.err_init;
+    stats[i].err_final = d.err_opt;
+    stats[i].rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
+    stats[i].solve_ms = aborted ? ms : (double)(d.t_end - d.t_begin) * 1e-6;  // this problem's own span
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
+                             cup2d_solve_stats* stats, void* stream) {
+  if (!B) return CUP2D_INVALID_ARGUMENT;
+  BatchArgs a;
+  int grid = 0, st;
+  if ((st = batch_prepare(B, d_b, d_x, B->d_p64.p, B->d_pmx.p, a, grid))) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = (int)B->probs.size();
+  const bool mixed = B->opts.precision == CUP2D_PREC_MIXED;
+  if ((mixed ? cudaMemcpyAsync(B->d_pmx.p, B->h_pmx.data(), sizeof(ProblemMixed) * n, cudaMemcpyHostToDevice, s)
+             : cudaMemcpyAsync(B->d_p64.p, B->h_p64.data(), sizeof(Problem64) * n, cudaMemcpyHostToDevice, s)) !=
+      cudaSuccess)
+    return CUP2D_CUDA_ERROR;
   if (B->profiling) {
     const int64_t words = (int64_t)grid * kProfPhases * 2;
     if ((st = B->prof.ensure(words))) return st;
@@ -916,7 +1000,7 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
     a.prof = B->prof.p;
   }
   if (stats) cudaEventRecord(B->ev0, s);
-  const cudaError_t e = launch_bicgstab_batch(a, grid, mixed, s);
+  const cudaError_t e = batch_enqueue(B, a, grid, grid / a.team, s);
   if (e != cudaSuccess) return from_cuda(e);
   if (!stats) return CUP2D_OK;
   cudaEventRecord(B->ev1, s);
@@ -930,18 +1014,160 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
   cudaEventElapsedTime(&ms, B->ev0, B->ev1);
   B->last_ms = ms;
   B->have_timeline = !aborted;
-  for (int i = 0; i < n; ++i) {
-    const DevStats& d = B->hstats[i];
-    stats[i].status = aborted ? CUP2D_TIMEOUT : d.status;
-    stats[i].iterations = d.iterations;
-    stats[i].restarts = d.restarts;
-    stats[i].refinements = d.refinements;
-    stats[i].err_init = d.err_init;
-    stats[i].err_final = d.err_opt;
-    stats[i].rel_res_inf = d.err_init > 0 ? d.err_opt / d.err_init : 0.0;
-    stats[i].solve_ms = aborted ? ms : (double)(d.t_end - d.t_begin) * 1e-6;  // this problem's own span
-  }
+  batch_fill_stats(B->hstats.data(), n, aborted, ms, stats);
   return aborted ? CUP2D_TIMEOUT : CUP2D_OK;
+}
+
+int cup2d_batch_capture(cup2d_batch* B, const double* const* d_b, double* const* d_x, int32_t flags) {
+  if (!B || (flags & ~CUP2D_GRAPH_ZERO_X)) return CUP2D_INVALID_ARGUMENT;
+  BatchGraph& g = B->graph;
+  if (g.replayed && cudaEventSynchronize(g.done) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  g.reset();
+  const int n = (int)B->probs.size();
+  const bool mixed = B->opts.precision == CUP2D_PREC_MIXED;
+  int st;
+  if ((st = mixed ? g.pmx.ensure(n) : g.p64.ensure(n))) return st;
+  BatchArgs a;
+  int grid = 0;
+  if ((st = batch_prepare(B, d_b, d_x, g.p64.p, g.pmx.p, a, grid))) return st;
+  if (!g.hstats && cudaMallocHost(&g.hstats, sizeof(DevStats) * n + sizeof(int)) != cudaSuccess) {
+    g.hstats = nullptr;
+    return CUP2D_OOM;
+  }
+  g.habort = reinterpret_cast<int*>(g.hstats + n);
+  // the graph's own descriptors: solves outside the graph keep theirs
+  cudaStream_t s = B->stream;
+  if ((mixed ? cudaMemcpyAsync(g.pmx.p, B->h_pmx.data(), sizeof(ProblemMixed) * n, cudaMemcpyHostToDevice, s)
+             : cudaMemcpyAsync(g.p64.p, B->h_p64.data(), sizeof(Problem64) * n, cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  cudaError_t e = cudaSuccess;
+  if (flags & CUP2D_GRAPH_ZERO_X)
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+      e = cudaMemsetAsync(d_x[i], 0, sizeof(double) * B->probs[i]->nb * kBLEN, s);
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(B->ev0, s, cudaEventRecordExternal);
+  if (e == cudaSuccess) e = batch_enqueue(B, a, grid, grid / a.team, s);
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(B->ev1, s, cudaEventRecordExternal);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g.hstats, B->dstats.p, sizeof(DevStats) * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g.habort, B->abort_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    g.exec = nullptr;
+    return from_cuda(e);
+  }
+  g.n = n;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_replay(cup2d_batch* B, void* stream) {
+  if (!B || !B->graph.exec) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaGraphLaunch(B->graph.exec, s) != cudaSuccess || cudaEventRecord(B->graph.done, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  B->graph.replayed = true;
+  return CUP2D_OK;
+}
+
+int cup2d_batch_replay_stats(cup2d_batch* B, cup2d_solve_stats* stats) {
+  if (!B || !B->graph.exec || !B->graph.replayed || !stats) return CUP2D_INVALID_ARGUMENT;
+  BatchGraph& g = B->graph;
+  if (cudaEventSynchronize(g.done) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, B->ev0, B->ev1);
+  B->last_ms = ms;
+  const int aborted = *g.habort;
+  B->have_timeline = !aborted;
+  std::memcpy(B->hstats.data(), g.hstats, sizeof(DevStats) * g.n);
+  batch_fill_stats(g.hstats, g.n, aborted, ms, stats);
+  return aborted ? CUP2D_TIMEOUT : CUP2D_OK;
+}
+
+int cup2d_batch_tune(cup2d_batch* B, const double* const* d_b, double* const* d_x, const int32_t* teams,
+                     int32_t nteams, const int32_t* ctas_per_sm, int32_t ncps, int32_t iters, double* rates,
+                     int32_t* best_team, int32_t* best_ctas_per_sm) {
+  if (!B || !d_b || !d_x || !teams || nteams < 1 || iters < 0 || !best_team) return CUP2D_INVALID_ARGUMENT;
+  if (ncps < 0 || (ncps > 0 && !ctas_per_sm)) return CUP2D_INVALID_ARGUMENT;
+  const cup2d_solve_opts saved = B->opts;
+  const int saved_team = B->team, saved_cps = B->ctas_per_sm;
+  const int n = (int)B->probs.size();
+  std::vector<double*> x0;  // full solves: every candidate starts from the caller's x
+  if (iters > 0) {          // fixed work: every problem runs exactly `iters` iterations
+    cup2d_solve_opts o = saved;
+    o.tol_abs = 0.0;
+    o.tol_rel = 0.0;
+    o.max_iter = iters;
+    o.max_restarts = std::max(o.max_restarts, iters + 1);
+    B->opts = o;
+  } else {
+    for (int i = 0; i < n; ++i) {
+      double* c = nullptr;
+      const size_t bytes = sizeof(double) * B->probs[i]->nb * kBLEN;
+      if (!d_x[i] || cudaMallocAsync(reinterpret_cast<void**>(&c), bytes, B->stream) != cudaSuccess ||
+          cudaMemcpyAsync(c, d_x[i], bytes, cudaMemcpyDeviceToDevice, B->stream) != cudaSuccess) {
+        cudaGetLastError();
+        for (double* q : x0) cudaFreeAsync(q, B->stream);
+        if (c) cudaFreeAsync(c, B->stream);
+        cudaStreamSynchronize(B->stream);
+        return d_x[i] ? CUP2D_OOM : CUP2D_INVALID_ARGUMENT;
+      }
+      x0.push_back(c);
+    }
+  }
+  auto restart_x = [&]() {
+    for (int i = 0; i < (int)x0.size(); ++i)
+      cudaMemcpyAsync(d_x[i], x0[i], sizeof(double) * B->probs[i]->nb * kBLEN, cudaMemcpyDeviceToDevice,
+                      B->stream);
+  };
+  std::vector<cup2d_solve_stats> st(n);
+  double best_rate = -1.0;
+  int best = saved_team, best_cps = saved_cps, status = CUP2D_OK;
+  const int nc = std::max(ncps, 1);
+  for (int k = 0; k < nteams && status == CUP2D_OK; ++k) {
+    for (int c = 0; c < nc; ++c) {
+      const int cps = ncps > 0 ? ctas_per_sm[c] : saved_cps;
+      if (teams[k] < 1 || teams[k] > 256 || cps < 0 || cps > 32) {
+        status = CUP2D_INVALID_ARGUMENT;
+        break;
+      }
+      B->team = teams[k];
+      B->ctas_per_sm = cps;
+      double rate = 0.0;
+      restart_x();
+      int s = cup2d_batch_solve_device(B, d_b, d_x, st.data(), B->stream);  // warm-up
+      restart_x();
+      if (s == CUP2D_OK) s = cup2d_batch_solve_device(B, d_b, d_x, st.data(), B->stream);
+      if (s == CUP2D_OK && B->last_ms > 0.f) {
+        double work = 0.0;
+        for (int i = 0; i < n; ++i) work += (double)st[i].iterations * (double)B->probs[i]->nb * kBLEN;
+        rate = work / (1e-3 * B->last_ms);
+      } else if (s != CUP2D_OK && s != CUP2D_INVALID_ARGUMENT) {
+        status = s;
+        break;
+      }
+      if (rates) rates[k * nc + c] = rate;
+      if (rate > best_rate) {
+        best_rate = rate;
+        best = teams[k];
+        best_cps = cps;
+      }
+    }
+  }
+  for (double* q : x0) cudaFreeAsync(q, B->stream);
+  cudaStreamSynchronize(B->stream);
+  B->opts = saved;
+  B->team = status == CUP2D_OK ? best : saved_team;
+  B->ctas_per_sm = status == CUP2D_OK ? best_cps : saved_cps;
+  *best_team = B->team;
+  if (best_ctas_per_sm) *best_ctas_per_sm = B->ctas_per_sm;
+  return status;
 }
 
 int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x, cup2d_solve_stats* stats) {

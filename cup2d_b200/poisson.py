@@ -260,6 +260,85 @@ class BatchSolver:
             return self.last_stats
         return None
 
+    def set_occupancy(self, ctas_per_sm: int) -> None:
+        """CTAs per SM of batched launches (0 = as many as fit)."""
+        L.check(L.lib().cup2d_batch_set_occupancy(self._h, int(ctas_per_sm)), "cup2d_batch_set_occupancy")
+
+    def autotune(self, bs, xs, teams=(4, 8, 12, 16, 24, 32), ctas_per_sm=(0, 2), iters: int = 30,
+                 cache: Optional[str] = None) -> tuple[int, int]:
+        """Picks the launch shape for this batch -- team size (CTAs per
+        problem) and occupancy cap (CTAs per SM, 0 = all that fit): every
+        candidate pair runs a batched launch with each problem capped at
+        `iters` iterations, the fastest in cell-iterations/s is kept and
+        returned as (team, ctas_per_sm).  With `cache` (a JSON file) a choice
+        made before for the same GPU, precision and size distribution is
+        reused without timing.  xs are overwritten when timing runs."""
+        import json
+        import os
+
+        import torch
+        sizes = np.sort([self.ncells(i) // 64 for i in range(len(self))])
+        key = "|".join([torch.cuda.get_device_name(), "mixed" if self.opts.precision == L.PREC_MIXED else "fp64",
+                        f"n={len(sizes)}", "q=" + ",".join(str(int(sizes[int(q * (len(sizes) - 1))]))
+                                                              for q in (0.1, 0.5, 0.9, 1.0)),
+                        "teams=" + ",".join(map(str, teams)), "cps=" + ",".join(map(str, ctas_per_sm))])
+        table = {}
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                table = json.load(f)
+            if key in table:
+                team, cps = int(table[key]["team"]), int(table[key]["ctas_per_sm"])
+                self.set_team(team)
+                self.set_occupancy(cps)
+                return team, cps
+        n = len(self)
+        for i in range(n):
+            _check_dev(bs[i], self.ncells(i))
+            _check_dev(xs[i], self.ncells(i))
+        pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
+        px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
+        ct = (C.c_int32 * len(teams))(*teams)
+        cc = (C.c_int32 * max(1, len(ctas_per_sm)))(*ctas_per_sm)
+        rates = (C.c_double * (len(teams) * max(1, len(ctas_per_sm))))()
+        best, best_cps = C.c_int32(), C.c_int32()
+        L.check(L.lib().cup2d_batch_tune(self._h, pb, px, ct, len(teams), cc, len(ctas_per_sm), int(iters), rates,
+                                         C.byref(best), C.byref(best_cps)), "cup2d_batch_tune")
+        nc = max(1, len(ctas_per_sm))
+        cps_list = list(ctas_per_sm) if ctas_per_sm else [0]
+        self.tune_rates = {(t, cps_list[c]): rates[k * nc + c] for k, t in enumerate(teams) for c in range(nc)}
+        if cache:
+            table[key] = {"team": best.value, "ctas_per_sm": best_cps.value,
+                          "rates": {f"{t}/{c}": r for (t, c), r in self.tune_rates.items()}}
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            with open(cache, "w") as f:
+                json.dump(table, f, indent=1)
+        return best.value, best_cps.value
+
+    def capture(self, bs, xs, zero_x: bool = False) -> None:
+        """Records one whole batched solve of these device tensors as a CUDA
+        graph (options, team and occupancy as now); `replay` then re-runs it
+        on whatever bs/xs hold, with xs warm from the previous replay unless
+        zero_x.  The tensors are kept alive while the graph exists."""
+        n = len(self)
+        if len(bs) != n or len(xs) != n:
+            raise ValueError(f"expected {n} right-hand sides and solutions")
+        for i in range(n):
+            _check_dev(bs[i], self.ncells(i))
+            _check_dev(xs[i], self.ncells(i))
+        pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
+        px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
+        L.check(L.lib().cup2d_batch_capture(self._h, pb, px, L.GRAPH_ZERO_X if zero_x else 0), "cup2d_batch_capture")
+        self._graph_io = (list(bs), list(xs))
+
+    def replay(self, stream=None) -> None:
+        L.check(L.lib().cup2d_batch_replay(self._h, _stream_handle(stream)), "cup2d_batch_replay")
+
+    def replay_stats(self) -> list[dict]:
+        st = (L.SolveStats * len(self))()
+        L.check(L.lib().cup2d_batch_replay_stats(self._h, st), "cup2d_batch_replay_stats")
+        self.last_stats = [s.as_dict() for s in st]
+        return self.last_stats
+
     def solve(self, bs, xs) -> list[dict]:
         """Host arrays (contiguous float64, e.g. pinned): xs[i] holds the
         initial guess and receives the solution; the copies are part of the

@@ -196,6 +196,35 @@ int64_t cup2d_batch_num_cells(const cup2d_batch* B, int32_t i);
  * launch, from its team taking it to its solution written). */
 int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* const* d_x,
                              cup2d_solve_stats* stats, void* stream);
+/* CTAs per SM of batched launches (the occupancy cap, 0..32; 0 = as many
+ * as fit, the default): smaller caps trade latency hiding for fewer
+ * barrier parties and less L2 pressure. */
+int cup2d_batch_set_occupancy(cup2d_batch* B, int32_t ctas_per_sm);
+/* Autotuner for the launch shape: times a batched launch of every pair
+ * (teams[k], ctas_per_sm[c]) -- each problem capped at `iters` iterations,
+ * so every candidate does the same work, or with iters = 0 full solves to
+ * the batch's tolerance, each from the caller's x; one warm-up launch each
+ * -- writes the rates in cell-iterations/s to rates[k*max(ncps,1) + c] (0
+ * where the pair does not fit the device), keeps the fastest pair for later
+ * solves and returns it.  ncps = 0 tunes the team alone at the current
+ * occupancy cap.  x is overwritten. */
+int cup2d_batch_tune(cup2d_batch* B, const double* const* d_b, double* const* d_x, const int32_t* teams,
+                     int32_t nteams, const int32_t* ctas_per_sm, int32_t ncps, int32_t iters, double* rates,
+                     int32_t* best_team, int32_t* best_ctas_per_sm);
+/* CUDA-graph form of a batched solve, for repeated solves on the same
+ * device buffers (time stepping: new b in place, x warm from the last step).
+ * cup2d_batch_capture records one whole solve of d_b/d_x -- state resets,
+ * with CUP2D_GRAPH_ZERO_X zeroing every x first, the persistent launch, the
+ * read-back of the statistics -- with the options, team and occupancy cap
+ * in force at capture time; a new capture replaces the old graph.
+ * cup2d_batch_replay enqueues one replay on `stream` (asynchronous);
+ * cup2d_batch_replay_stats waits for the last replay and fills stats[0..n-1]
+ * as cup2d_batch_solve_device does.  One solve or replay of a batch may be
+ * in flight at a time. */
+#define CUP2D_GRAPH_ZERO_X 1
+int cup2d_batch_capture(cup2d_batch* B, const double* const* d_b, double* const* d_x, int32_t flags);
+int cup2d_batch_replay(cup2d_batch* B, void* stream);
+int cup2d_batch_replay_stats(cup2d_batch* B, cup2d_solve_stats* stats);
 /* Same on host buffers (b[i] the RHS, x[i] initial guess in, solution out);
  * the copies are part of the call, on the batch's own stream. */
 int cup2d_batch_solve(cup2d_batch* B, const double* const* b, double* const* x,

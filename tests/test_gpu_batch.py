@@ -125,3 +125,80 @@ def test_batch_arguments(cuda):
             B.solve_device(bs, [xs[1], xs[0], xs[2]])  # sizes differ
     with pytest.raises(Cup2dError):
         BatchSolver([])
+
+
+def test_batch_autotune(cuda, tmp_path):
+    """The autotuner keeps the fastest candidate launch shape, the batch then
+    solves with it, and a second call with the same cache reuses the choice
+    without timing."""
+    import torch
+    bs, xs = _device_rhs(torch, cuda, MESHES)
+    cache = str(tmp_path / "tune.json")
+    with BatchSolver(MESHES, tol_rel=1e-6, precision="mixed") as B:
+        best = B.autotune(bs, xs, teams=(1, 2, 4, 8), ctas_per_sm=(0, 1), iters=10, cache=cache)
+        rates = B.tune_rates
+        assert best in rates and rates[best] == max(rates.values()) and rates[best] > 0
+        assert len(rates) == 8
+        # the chosen team is in use: results equal a single solve on that grid
+        for x in xs:
+            x.zero_()
+        st = B.solve_device(bs, xs)
+    assert all(s["status"] == L.OK for s in st)
+    with Solver(MESHES[2], tol_rel=1e-6, precision="mixed") as s1:
+        s1.set_grid(best[0])
+        x1 = torch.zeros_like(bs[2])
+        s1.solve_device(bs[2], x1)
+    assert torch.equal(x1, xs[2])
+    with BatchSolver(MESHES, tol_rel=1e-6, precision="mixed") as B2:
+        assert B2.autotune(bs, xs, teams=(1, 2, 4, 8), ctas_per_sm=(0, 1), iters=10, cache=cache) == best
+        assert not hasattr(B2, "tune_rates")
+
+
+def test_batch_occupancy_cap(cuda):
+    """An occupancy cap changes how many problems run at once, never a
+    problem's result."""
+    import torch
+    bs, xs = _device_rhs(torch, cuda, MESHES)
+    with BatchSolver(MESHES, tol_rel=1e-8, max_iter=5000, team=4) as B:
+        B.solve_device(bs, xs)
+        ys = [torch.zeros_like(b) for b in bs]
+        B.set_occupancy(1)
+        B.solve_device(bs, ys)
+        with pytest.raises(Cup2dError):
+            B.set_occupancy(-1)
+    assert all(torch.equal(x, y) for x, y in zip(xs, ys))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_graph_replay(cuda, precision):
+    """A captured batch replays to the same results as solve_device: cold
+    (x zeroed inside the graph) with the captured b, and after b is
+    overwritten in place, warm from the previous replay's x."""
+    import torch
+    bs, xs = _device_rhs(torch, cuda, MESHES)
+    tol = dict(tol_rel=1e-8, max_iter=5000, precision=precision, team=4)
+    with BatchSolver(MESHES, **tol) as B:
+        ref = B.solve_device(bs, [torch.zeros_like(b) for b in bs])
+        xref = [torch.zeros_like(b) for b in bs]
+        B.solve_device(bs, xref)
+        B.capture(bs, xs, zero_x=True)
+        for x in xs:
+            x.fill_(1.0)  # zeroed by the graph
+        for _ in range(2):
+            B.replay()
+            st = B.replay_stats()
+            assert [s["iterations"] for s in st] == [s["iterations"] for s in ref]
+            assert all(torch.equal(x, y) for x, y in zip(xs, xref))
+        # time stepping: new b in place, warm start from the last solution
+        B.capture(bs, xs)
+        warm = [x.clone() for x in xs]
+        for b, m, i in zip(bs, MESHES, range(len(bs))):
+            b.copy_(torch.from_numpy(m.rhs_fourier(900 + i)))
+        B.replay()
+        st = B.replay_stats()
+        assert all(s["status"] == L.OK for s in st)
+        B.solve_device(bs, warm)
+        assert all(torch.equal(x, y) for x, y in zip(xs, warm))
+    with pytest.raises(Cup2dError):
+        with BatchSolver(MESHES[:2], **tol) as B2:
+            B2.replay()
