@@ -151,6 +151,47 @@ def algorithmic_bytes(n: int, nb: int, R: int, nnz: int, iters: int, updates: in
     return setup + iters * per_iter + updates * per_update + final
 
 
+def spmv_leg(dev, stream, steps: int = 20, warmup: int = 5) -> dict:
+    """The operator apply y = A x alone (the library's standalone SpMV, FP64
+    and FP32) on one forest far above L2: bpdx=64, bpdy=32, levelMax=6, 3
+    seeded disks, band 0.35 (1.15 M blocks, 73 M cells: 1.2 GB of x and y in
+    FP64, so that launch and ramp-up are small against the transfer).
+    Algorithmic bytes per launch:
+    read x, write y, the explicit coarse/fine rows (values + column indices +
+    row pointers) and 28 B of block structure per block."""
+    import numpy as np
+    import torch
+
+    from cup2d_b200 import Mesh, Solver
+    from cup2d_b200.problems import EXTENT, seeded_disks
+    mesh = Mesh.disks(64, 32, 6, EXTENT, seeded_disks(np.random.default_rng(5), 3), 0.35)
+    n = mesh.ncells
+    out = {"mesh": f"bpdx=64 bpdy=32 levelMax=6, 3 disks, band 0.35: {mesh.nblocks} blocks, {n} cells"}
+    peak, kind = _peaks()
+    with Solver(mesh) as h:
+        R, nnz = h.explicit_info()
+        for name, dt, vb, ab in (("fp64", torch.float64, 8, 12.0), ("fp32", torch.float32, 4, 8.0)):
+            g = torch.Generator(device=dev).manual_seed(1)
+            x = torch.randn(n, dtype=dt, device=dev, generator=g)
+            y = torch.empty_like(x)
+            ms = []
+            for i in range(warmup + steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                h.apply(x, y, stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                if i >= warmup:
+                    ms.append(e0.elapsed_time(e1))
+            by = 2.0 * vb * n + ab * nnz + 4.0 * R + 28.0 * mesh.nblocks
+            t = statistics.median(ms)
+            out[name] = {"kernel": "k_apply", "ms": t, "bytes": by, "achieved": by / (t * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": by / (t * 1e-3) / 1e9 / peak, "peak_kind": kind,
+                         "l2": "x and y larger than L2" if 2 * vb * n > 126e6 else "x and y fit in L2"}
+    return out
+
+
 def run_ours(args, world, rank, local) -> dict | None:
     """Single-problem workloads (large, small): a step is one solve."""
     import numpy as np
@@ -433,6 +474,7 @@ def run_batch(args, world, rank, local) -> dict | None:
         B.solve(hbn, hxn)
     e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
     B.close()
+    spmv = spmv_leg(dev, stream) if not args.no_spmv else None
 
     K = args.steps
     tot_mx = _max_over_ranks(sum(ms_mx), world)
@@ -492,6 +534,7 @@ def run_batch(args, world, rank, local) -> dict | None:
                      "peak_kind": peak_kind},
         "e2e": {"value": world * n * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * sum(cells),
                 "d2h_bytes_per_step": 8 * sum(cells)},
+        "spmv": spmv,
         "gpu_launches": K,
         "clocks": clk.summary(),
         "status_ok": all(s["status"] == 0 for s in st_mx + st_b64),
@@ -508,6 +551,85 @@ def run_batch(args, world, rank, local) -> dict | None:
                       f"range ({tot:.1f} s, OpenMP, {cores} threads): {sec * 1e9:.2f} ns per cell-iteration, scaled "
                       f"by the FP64 cell-iterations of this batch ({cit_64 / n:.3g} per solve)"}
     return line
+
+
+def run_timestep(args) -> dict:
+    """Time-stepping sequence: `--ts-steps` consecutive solves on the large
+    forest (bpdx=8, bpdy=4, levelMax=7, 3 seeded disks) whose disks move
+    0.002 per step along x; every 10 steps the forest is rebuilt on the host,
+    re-assembled on the device and the pressure carried over by the device
+    transfer.  The RHS comes from AR(1) Fourier coefficients (rho 0.95)
+    through the device RHS kernel; each solve is warm-started from the
+    previous pressure, to |b - Ax|_inf <= 1e-6 |b|_inf.  Run for the mixed and
+    the plain FP64 solver; wall-clock over the whole sequence (host forest
+    builds included) and CUDA-event solve times per step."""
+    import numpy as np
+    import torch
+
+    from cup2d_b200 import Solver
+    from cup2d_b200.mesh import fourier_advance, fourier_coefs
+    from cup2d_b200.problems import large_mesh
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    seed, every = 11, 10
+    out = {}
+
+    def sequence(precision: str, steps: int, warm: bool):
+        opts = dict(tol_rel=0.0, max_iter=20000, max_restarts=100, timeout_ms=120000, precision=precision)
+        mesh = large_mesh(1)
+        cur, spare = Solver(mesh, **opts), Solver(mesh, **opts)
+        coef = fourier_coefs(seed)
+        x = torch.zeros(mesh.ncells, dtype=torch.float64, device=dev)
+        b = torch.empty_like(x)
+        its, solve_ms, remesh_ms, nblocks = [], [], [], []
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for step in range(steps):
+            if step > 0 and step % every == 0:
+                tr = time.perf_counter()
+                mesh = large_mesh(1, shift_x=0.002 * step)
+                spare.update_mesh(mesh)
+                x_new = torch.empty(mesh.ncells, dtype=torch.float64, device=dev)
+                cur.transfer_to(spare, x, x_new, stream=stream)
+                cur, spare, x = spare, cur, x_new
+                b = torch.empty_like(x)
+                torch.cuda.synchronize(dev)
+                remesh_ms.append((time.perf_counter() - tr) * 1e3)
+            coef = fourier_advance(coef, seed, step)
+            cur.rhs_fourier_device(coef, b, stream=stream)
+            cur.set_opts(tol_abs=TOL * float(b.abs().max()), **opts)
+            if not warm:
+                x.zero_()
+            st = cur.solve_device(b, x, stream=stream)
+            if st["status"] != 0:
+                raise RuntimeError(f"step {step}: status {st['status']}")
+            its.append(st["iterations"])
+            solve_ms.append(st["solve_ms"])
+            nblocks.append(mesh.nblocks)
+        wall = time.perf_counter() - t0
+        cur.close()
+        spare.close()
+        return {"solves_per_s": steps / wall, "steps": steps, "wall_s": wall,
+                "solve_ms": {"p50": _pct(solve_ms, 0.5), "p99": _pct(solve_ms, 0.99),
+                             "mean": statistics.mean(solve_ms)},
+                "iterations_mean": statistics.mean(its),
+                "remesh_ms_mean": statistics.mean(remesh_ms) if remesh_ms else None,
+                "remeshes": len(remesh_ms), "blocks": [min(nblocks), max(nblocks)]}
+
+    sequence("mixed", min(args.warmup, 5), True)  # warm-up: library, allocator, clocks
+    with ClockSampler(0) as clk:
+        for prec in ("mixed", "fp64"):
+            out[prec] = sequence(prec, args.ts_steps, True)
+        out["mixed_cold"] = sequence("mixed", min(args.ts_steps, 50), False)
+    return {"metric": "time-stepping Poisson solves/s (warm start, remesh every 10 steps)",
+            "value": out["mixed"]["solves_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.ts_steps,
+            "warmup": min(args.warmup, 5), "higher_is_better": True, "dtype": "f32+f64",
+            "config": {"workload": "timestep: large forest (bpdx=8 bpdy=4 levelMax=7, 3 seeded disks), disks "
+                                   "move 0.002/step, remesh + device re-assembly + device pressure transfer "
+                                   "every 10 steps, AR(1) rho=0.95 Fourier RHS on the device, warm start",
+                       "tol": "|b - Ax|_inf <= 1e-6 |b|_inf per step"},
+            "legs": out, "clocks": clk.summary(), "data": "synthetic"}
 
 
 def run_serve(args) -> dict:
@@ -771,15 +893,19 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batch", "large", "small", "serve"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "large", "small", "serve", "timestep"], default="batch")
+    ap.add_argument("--ts-steps", type=int, default=500, help="timestep workload: time steps per leg")
     ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
     ap.add_argument("--team-mixed", type=int, default=16, help="batch: CTAs per problem, mixed")
     ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64")
     ap.add_argument("--no-tune", action="store_true", help="batch: fixed teams, no autotuner")
-    ap.add_argument("--tune-iters", type=int, default=40,
-                    help="batch autotuner: iterations per problem of a candidate (0 = full solves)")
-    ap.add_argument("--tune-teams", default="8,12,16,24,32", help="batch autotuner: candidate teams")
-    ap.add_argument("--tune-cps", default="0,2", help="batch autotuner: candidate CTAs per SM (0 = all)")
+    ap.add_argument("--tune-iters", type=int, default=0,
+                    help="batch autotuner: iterations per problem of a candidate (0 = full solves: a fixed "
+                         "iteration count ignores the tail of the largest problems and favours small teams)")
+    ap.add_argument("--tune-teams", default="6,8,12,16", help="batch autotuner: candidate teams")
+    ap.add_argument("--tune-cps", default="0", help="batch autotuner: candidate CTAs per SM (0 = all)")
+    ap.add_argument("--no-spmv", action="store_true", help="batch: skip the standalone SpMV leg")
+    ap.add_argument("--spmv-only", action="store_true", help="the standalone SpMV leg alone (profiling runs)")
     ap.add_argument("--no-graph", action="store_true", help="batch: launch directly instead of graph replays")
     ap.add_argument("--plain-steps", type=int, default=3, help="batch: timed steps of the one-at-a-time FP64 leg")
     ap.add_argument("--cpu-iters", type=int, default=600, help="CPU baseline: iterations per sampled problem")
@@ -801,6 +927,12 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.profile_iters > 0:
         return profile_case(args)
+    if args.spmv_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps(spmv_leg(dev, torch.cuda.current_stream(dev), steps=args.steps, warmup=args.warmup)))
+        return 0
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
@@ -809,10 +941,10 @@ def main(argv=None) -> int:
         line = run_reference(args, world, rank)
     else:
         world, rank, local = _dist()
-        if args.workload == "serve":
+        if args.workload in ("serve", "timestep"):
             import torch
             torch.cuda.set_device(local)
-            line = run_serve(args) if rank == 0 else None
+            line = (run_serve if args.workload == "serve" else run_timestep)(args) if rank == 0 else None
         else:
             line = (run_batch if args.workload == "batch" else run_ours)(args, world, rank, local)
         if world > 1:

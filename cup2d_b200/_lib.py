@@ -93,6 +93,8 @@ SIGNATURES = {
     "cup2d_batch_tune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), P_i32, C.c_int32,
                                    P_i32, C.c_int32, C.c_int32, P_f64, P_i32, P_i32]),
     "cup2d_batch_set_occupancy": (C.c_int, [C.c_void_p, C.c_int32]),
+    "cup2d_poisson_rhs_fourier_device": (C.c_int, [C.c_void_p, C.c_int32, P_f64, C.c_void_p, C.c_void_p]),
+    "cup2d_poisson_transfer": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_batch_capture": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32]),
     "cup2d_batch_replay": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cup2d_batch_replay_stats": (C.c_int, [C.c_void_p, C.c_void_p]),

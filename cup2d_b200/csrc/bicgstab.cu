@@ -93,12 +93,6 @@ struct Smem {
 
 // max that propagates NaN (fmax drops it, which would let a blown-up
 // residual read as converged)
-// Start of part k of n equal parts of [0, total): 64-bit product, 32-bit
-// result (cell and block indices of one problem fit in 31 bits).
-__device__ __forceinline__ int share(long long total, unsigned k, unsigned n) {
-  return (int)(total * (long long)k / (long long)n);
-}
-
 __device__ __forceinline__ double nanmax(double a, double b) { return (a > b || a != a) ? a : b; }
 
 template <int NV>
@@ -979,43 +973,6 @@ cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cuda
 }
 
 // ------------------------------------------------------- single ops -------
-
-// y = A x with the solver's own SpMV (the range form of the passes): CTA c
-// takes an equal share of the blocks and of the explicit rows.
-template <class T>
-struct EpiY {
-  static constexpr int LV = Lane<T>::V;
-  T* y;
-  struct Pre {};
-  __device__ __forceinline__ Pre load(int) const { return Pre{}; }
-  __device__ __forceinline__ Pre load1(int) const { return Pre{}; }
-  __device__ __forceinline__ void vec(int i0, const T (&v)[LV], const Pre&) { stv<LV>(y + i0, v); }
-  __device__ __forceinline__ void one(int i, T v, const Pre&, int) { y[i] = v; }
-};
-
-template <class T>
-__global__ void __launch_bounds__(kSolveThreads) k_apply(MeshView M, const T* __restrict__ x, T* __restrict__ y) {
-  const int b0 = share(M.nb, blockIdx.x, gridDim.x), b1 = share(M.nb, blockIdx.x + 1, gridDim.x);
-  const int r0 = share(M.R, blockIdx.x, gridDim.x), r1 = share(M.R, blockIdx.x + 1, gridDim.x);
-  EpiY<T> epi{y};
-  spmv_range<T>(M, x, b0, b1, r0, r1, epi);
-}
-
-template <class T>
-cudaError_t launch_apply(const MeshView& M, const T* x, T* y, cudaStream_t s) {
-  if (M.nb <= 0) return cudaSuccess;
-  const int ctas = (M.nb + 15) / 16;
-  k_apply<T><<<(unsigned)(ctas < 65535 ? ctas : 65535), kSolveThreads, 0, s>>>(M, x, y);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s) {
-  return launch_apply<double>(M, x, y, s);
-}
-
-cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, cudaStream_t s) {
-  return launch_apply<float>(M, x, y, s);
-}
 
 __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int nb,
                                                              const double* __restrict__ p, double* __restrict__ z) {

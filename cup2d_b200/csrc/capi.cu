@@ -171,6 +171,7 @@ struct cup2d_poisson {
   DevBuf<int> abort_flag;
   DevBuf<DevStats> dstats;
   DevBuf<unsigned long long> prof;  // phase timers (profiling on)
+  DevBuf<double> rhs_coef, rhs_part;  // device RHS: coefficients, partial sums + mean
   uint64_t mesh_version = 0;
   bool profiling = false;
   int prof_grid = 0;                // grid of the profiled solves
@@ -450,7 +451,7 @@ int handle_destroy_idle(cup2d_poisson* h) {
   for (auto* b : i32) b->release();
   h->xmask.release();
   DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->xo, &h->r, &h->rh, &h->p, &h->nu, &h->t,
-                           &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
+                           &h->z, &h->z2, &h->bstage, &h->xstage, &h->red, &h->rhs_coef, &h->rhs_part};
   for (auto* b : f64) b->release();
   DevBuf<float>* f32[] = {&h->xval32, &h->f_r, &h->f_rh, &h->f_p,
                           &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
@@ -570,13 +571,66 @@ int cup2d_poisson_solve(cup2d_poisson* h, const double* b, double* x, cup2d_solv
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream) {
   if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
-  return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, s));
+  return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, h->err.p, s));
 }
 
 int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream) {
   if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
-  return from_cuda(launch_spmv32(h->mesh.view(), d_x, d_y, s));
+  return from_cuda(launch_spmv32(h->mesh.view(), d_x, d_y, h->err.p, s));
+}
+
+}  // extern "C"
+
+namespace {
+
+ForestView forest_view(const cup2d_poisson* h) {
+  ForestView F{};
+  F.bpdx = h->bpdx;
+  F.bpdy = h->bpdy;
+  F.L = h->level_max;
+  F.nb = h->nb;
+  F.h0 = h->extent / ((double)std::max(h->bpdx, h->bpdy) * 8.0);
+  F.level = h->level.p;
+  F.bx = h->bx.p;
+  F.by = h->by.p;
+  F.table = h->table.p;
+  int64_t off = 0;
+  for (int l = 0; l < h->level_max; ++l) {
+    F.off[l] = off;
+    off += ((int64_t)h->bpdx << l) * ((int64_t)h->bpdy << l);
+  }
+  F.off[h->level_max] = off;
+  return F;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cup2d_poisson_rhs_fourier_device(cup2d_poisson* h, int32_t kmax, const double* coef, double* d_b,
+                                     void* stream) {
+  if (!h || !coef || !d_b || kmax < 1 || kmax > kMaxFourierK || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int nm = fourier_mode_count(kmax);
+  int st;
+  if ((st = h->rhs_coef.ensure(4 * nm)) || (st = h->rhs_part.ensure(rhs_partials(h->nb) + 1))) return st;
+  if (cudaMemcpyAsync(h->rhs_coef.p, coef, sizeof(double) * 4 * nm, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  const int64_t parts = rhs_partials(h->nb);
+  return from_cuda(launch_rhs_fourier(forest_view(h), kmax, h->rhs_coef.p, d_b, h->rhs_part.p,
+                                      h->rhs_part.p + parts, s));
+}
+
+int cup2d_poisson_transfer(const cup2d_poisson* src, const double* d_xsrc, const cup2d_poisson* dst, double* d_xdst,
+                           void* stream) {
+  if (!src || !dst || !d_xsrc || !d_xdst || d_xsrc == d_xdst || src->nb <= 0 || dst->nb <= 0)
+    return CUP2D_INVALID_ARGUMENT;
+  if (src->bpdx != dst->bpdx || src->bpdy != dst->bpdy || src->extent != dst->extent)
+    return CUP2D_INVALID_ARGUMENT;  // not the same domain and root grid
+  if (std::max(src->level_max, dst->level_max) + 1 + 3 + 7 > 62) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return from_cuda(launch_transfer(forest_view(src), d_xsrc, forest_view(dst), d_xdst, s));
 }
 
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream) {
@@ -1249,7 +1303,8 @@ int64_t handle_bytes(const cup2d_poisson* h) {
   for (auto* b : i32) n += b->cap * (int64_t)sizeof(int32_t);
   n += h->xmask.cap * (int64_t)sizeof(unsigned long long);
   const DevBuf<double>* f64[] = {&h->hblk, &h->xval, &h->xo, &h->r, &h->rh, &h->p, &h->nu,
-                                 &h->t, &h->z, &h->z2, &h->bstage, &h->xstage, &h->red};
+                                 &h->t, &h->z, &h->z2, &h->bstage, &h->xstage, &h->red, &h->rhs_coef,
+                                 &h->rhs_part};
   for (auto* b : f64) n += b->cap * (int64_t)sizeof(double);
   const DevBuf<float>* f32[] = {&h->xval32, &h->f_r, &h->f_rh, &h->f_p, &h->f_nu, &h->f_t, &h->f_z, &h->f_z2};
   for (auto* b : f32) n += b->cap * (int64_t)sizeof(float);

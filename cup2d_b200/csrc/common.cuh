@@ -126,6 +126,12 @@ struct GridBarrier {
 
 __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
+// Start of part k of n equal parts of [0, total): 64-bit product, 32-bit
+// result (cell and block indices of one problem fit in 31 bits).
+__device__ __forceinline__ int share(long long total, unsigned k, unsigned n) {
+  return (int)(total * (long long)k / (long long)n);
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

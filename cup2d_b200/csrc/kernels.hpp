@@ -172,9 +172,36 @@ int max_coop_grid_batch(int device, bool mixed);
 cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s);
 
 // Single operations (tests, residual checks).
-cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, cudaStream_t s);
-cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, cudaStream_t s);
+// y = A x (spmv_staged.cu); *err raised if a staged copy did not complete.
+cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, int* err, cudaStream_t s);
+cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, int* err, cudaStream_t s);
 cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s);
 cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s);
+
+// Forest of a handle on the device: per-block level and coordinates, and the
+// per-level dense leaf tables (block id or -1, level l at off[l], row-major
+// with (bpdx << l) columns).
+struct ForestView {
+  int32_t bpdx, bpdy, L;
+  int64_t nb;
+  double h0;  // cell size at level 0
+  const int32_t* level;
+  const int32_t* bx;
+  const int32_t* by;
+  const int32_t* table;
+  int64_t off[kMaxLevels + 1];
+};
+
+// Time-stepping steps around the solve (timestep.cu).
+constexpr int kMaxFourierK = 24;
+int fourier_mode_count(int kmax);
+int64_t rhs_partials(int64_t nb);  // scratch doubles of launch_rhs_fourier
+// b = zero-sum RHS of the Fourier velocity field with coefficients coef
+// (device, 4 per mode); partial [rhs_partials(nb)] and mean [1] scratch.
+cudaError_t launch_rhs_fourier(const ForestView& F, int kmax, const double* coef, double* b, double* partial,
+                               double* mean, cudaStream_t s);
+// xd (on D) = xs (on S) carried across a change of forest.
+cudaError_t launch_transfer(const ForestView& S, const double* xs, const ForestView& D, double* xd,
+                            cudaStream_t s);
 
 }  // namespace cup2d

@@ -32,12 +32,6 @@ __device__ __forceinline__ int4 block_nbr(const MeshView& M, int blk) {
   return __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
 }
 
-template <class T>
-__device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, int blk, const int4& nb) {
-  if (nb.x == kExplicit || nb.y == kExplicit || nb.z == kExplicit || nb.w == kExplicit) return __ldg(M.xmask + blk);
-  return 0ull;
-}
-
 // ------------------------------------------------ 16-byte lane layout ----
 //
 // The range passes move 16 bytes per lane and access: V = 4 consecutive
@@ -228,15 +222,16 @@ __device__ __forceinline__ void fill_siblings(ChunkGather<T>& ga, ChunkGather<T>
   (void)L;
 }
 
+// xmask: the block's explicit-row mask (fetched with its neighbour table).
 template <class T, class Epi>
-__device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGather<T>& g, const Lane<T>& L,
-                                               int blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
+__device__ __forceinline__ void chunk_epilogue(const ChunkGather<T>& g, const Lane<T>& L, int blk, bool valid,
+                                               unsigned long long xmask, const typename Epi::Pre& pre, Epi& epi) {
   constexpr int V = Lane<T>::V;
   T y[V];
   stencil_chunk<T>(g, L, y);
   if (!valid) return;
   const int i0 = blk * kBLEN + L.cell0;
-  const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, g.nb) >> L.cell0) & ((1u << V) - 1u);
+  const unsigned mk = (unsigned)(xmask >> L.cell0) & ((1u << V) - 1u);
   if (mk == 0u) {
     epi.vec(i0, y, pre);
   } else {
@@ -258,9 +253,9 @@ __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGat
 // each cell of the ranges is handed over exactly once, by one thread, in no
 // particular order.  A warp takes spans of 2*CB consecutive blocks (two
 // chunks in flight), takes the halos of sibling blocks inside the span from
-// shuffles, and fetches the neighbour tables of its next span while it
-// computes the current one.  The explicit rows' offsets are fetched before
-// the stencil loop.
+// shuffles, and fetches the neighbour tables and explicit-row masks of its
+// next span while it computes the current one.  The explicit rows' offsets
+// are fetched before the stencil loop.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int b0, int b1,
                                            int r0, int r1, Epi& epi) {
@@ -281,8 +276,10 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
   auto nbr_of = [&](int blk) {
     return blk < b1 ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
   };
+  auto mask_of = [&](int blk) { return blk < b1 ? __ldg(M.xmask + blk) : 0ull; };
   int sp = w;
   int4 na = nbr_of(b0 + sp * SPAN + L.bl), nbb = nbr_of(b0 + sp * SPAN + CB + L.bl);
+  unsigned long long ma = mask_of(b0 + sp * SPAN + L.bl), mb = mask_of(b0 + sp * SPAN + CB + L.bl);
   for (; sp < nsp; sp += nw) {
     const int ba = b0 + sp * SPAN + L.bl, bb = ba + CB;
     const bool va = ba < b1, vb = bb < b1;
@@ -294,12 +291,15 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
     Pre pa{}, pb{};
     if (va) pa = epi.load(ba * kBLEN + L.cell0);
     if (vb) pb = epi.load(bb * kBLEN + L.cell0);
+    const unsigned long long cma = ma, cmb = mb;
     const int nxt = b0 + (sp + nw) * SPAN + L.bl;
     na = nbr_of(nxt);
     nbb = nbr_of(nxt + CB);
+    ma = mask_of(nxt);
+    mb = mask_of(nxt + CB);
     fill_siblings<T>(ga, gb, sa, sb, L, lane);
-    chunk_epilogue<T>(M, ga, L, ba, va, pa, epi);
-    chunk_epilogue<T>(M, gb, L, bb, vb, pb, epi);
+    chunk_epilogue<T>(ga, L, ba, va, cma, pa, epi);
+    chunk_epilogue<T>(gb, L, bb, vb, cmb, pb, epi);
   }
   for (; r < r1; r += blockDim.x) {
     const Pre pre = epi.load1(cell);

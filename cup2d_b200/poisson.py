@@ -155,6 +155,24 @@ class Solver:
         fn = L.lib().cup2d_poisson_apply32 if str(x.dtype) == "torch.float32" else L.lib().cup2d_poisson_apply
         L.check(fn(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s), "cup2d_poisson_apply")
 
+    def rhs_fourier_device(self, coef: np.ndarray, b, kmax: int = 8, stream=None) -> None:
+        """b (float64 CUDA tensor) = the zero-sum synthetic RHS of this
+        forest for Fourier coefficients `coef` (Mesh.rhs_from_coefs on the
+        device)."""
+        coef = np.ascontiguousarray(coef, dtype=np.float64)
+        _check_dev(b, self.ncells)
+        L.check(L.lib().cup2d_poisson_rhs_fourier_device(self._h, int(kmax), _pd(coef), C.c_void_p(b.data_ptr()),
+                                                         _stream_handle(stream)), "cup2d_poisson_rhs_fourier_device")
+
+    def transfer_to(self, dst: "Solver", x_src, x_dst, stream=None) -> None:
+        """x_dst (on dst's forest) = x_src (on this forest), e.g. a warm
+        start carried across a mesh adaptation."""
+        _check_dev(x_src, self.ncells)
+        _check_dev(x_dst, dst.ncells)
+        L.check(L.lib().cup2d_poisson_transfer(self._h, C.c_void_p(x_src.data_ptr()), dst._h,
+                                               C.c_void_p(x_dst.data_ptr()), _stream_handle(stream)),
+                "cup2d_poisson_transfer")
+
     def precond(self, p, z, stream=None) -> None:
         fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond
         s = _stream_handle(stream)
@@ -264,12 +282,14 @@ class BatchSolver:
         """CTAs per SM of batched launches (0 = as many as fit)."""
         L.check(L.lib().cup2d_batch_set_occupancy(self._h, int(ctas_per_sm)), "cup2d_batch_set_occupancy")
 
-    def autotune(self, bs, xs, teams=(4, 8, 12, 16, 24, 32), ctas_per_sm=(0, 2), iters: int = 30,
+    def autotune(self, bs, xs, teams=(6, 8, 12, 16), ctas_per_sm=(0,), iters: int = 0,
                  cache: Optional[str] = None) -> tuple[int, int]:
         """Picks the launch shape for this batch -- team size (CTAs per
         problem) and occupancy cap (CTAs per SM, 0 = all that fit): every
-        candidate pair runs a batched launch with each problem capped at
-        `iters` iterations, the fastest in cell-iterations/s is kept and
+        candidate pair runs a batched launch -- full solves from xs with
+        iters = 0 (the default: the schedule's tail, set by the largest
+        problems, is part of the cost), or each problem capped at `iters`
+        iterations -- and the fastest in cell-iterations/s is kept and
         returned as (team, ctas_per_sm).  With `cache` (a JSON file) a choice
         made before for the same GPU, precision and size distribution is
         reused without timing.  xs are overwritten when timing runs."""

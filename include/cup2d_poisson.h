@@ -152,6 +152,23 @@ int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, doub
  * apply is the solver's own SpMV, in FP64 and in the FP32 of the mixed form. */
 int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* stream);
 int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream);
+/* Time-stepping steps around the solve, on the device.
+ * rhs_fourier_device: d_b = the zero-sum RHS of the synthetic pressure
+ * problem on the handle's forest, 0.5 h (u(x+h)-u(x-h) + v(y+h)-v(y-h)) of
+ * the Fourier velocity with host coefficients `coef` (cup2d_fourier_coefs /
+ * cup2d_fourier_advance layout, kmax 1..24) -- the device counterpart of
+ * cup2d_rhs_from_coefs, equal to it to rounding (CUP2D computes the RHS
+ * from the velocity field in updatePressureRHS,
+ * source/Operators/PressureSingle.cpp:324-456).
+ * transfer: d_xdst (on dst's forest) = d_xsrc (on src's forest), for a warm
+ * start across a mesh adaptation: same-level cells copied, a finer dst cell
+ * takes the coarse src cell holding its centre, a coarser dst cell the mean
+ * of the src cells at its four quadrant centres.  Both forests must share
+ * bpdx, bpdy and extent.  Asynchronous on `stream`. */
+int cup2d_poisson_rhs_fourier_device(cup2d_poisson* h, int32_t kmax, const double* coef, double* d_b,
+                                     void* stream);
+int cup2d_poisson_transfer(const cup2d_poisson* src, const double* d_xsrc, const cup2d_poisson* dst,
+                           double* d_xdst, void* stream);
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
 /* FP32 P^-1 apply of the mixed form (split-TF32 tensor-core MMA). */
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);
