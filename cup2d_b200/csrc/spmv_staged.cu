@@ -11,10 +11,12 @@
 //   tile i+2  the halos: the edge row or column of every same-level
 //             neighbour outside the tile across each face (cp.async,
 //             addresses from the table staged earlier);
-//   tile i    the 5-point rows from shared memory with the solver's lane
-//             layout and register stencil (spmv.cuh), so both SpMVs give
-//             the same bits; a face whose neighbour is in the same tile
-//             reads it there.
+//   tile i    the 5-point rows from shared memory in the solver's 16-byte
+//             lane layout (spmv.cuh): a lane's cells and the rows above and
+//             below are 16-byte shared loads, the neighbours across a face
+//             come from the same tile or the halo (address chosen without a
+//             branch); summed left, right, below, above and minus n z as the
+//             solver's SpMV does, so both give the same bits.
 // The explicit (coarse/fine) rows follow, CSR, as in the solver's passes.
 //
 // Every wait on a bulk copy is bounded (2 s of globaltimer): past it the CTA
@@ -157,26 +159,28 @@ __global__ void __launch_bounds__(kThreads) k_apply_staged(MeshView M, const T* 
       cp_async<8>(&sm.mask[i % kStages][tid], M.xmask + blk);
     }
   };
-  // halos of tile i from its staged table: per block 16 column values (x
-  // faces) and the 16-byte pieces of two rows (y faces), for neighbours
-  // outside the tile
+  // halos of tile i from its staged table, one thread per (block, face)
+  // whose neighbour is outside the tile: 8 column values for an x face, the
+  // 16-byte pieces of a row for a y face
   auto issue_halos = [&](int i) {
     if (i >= ntiles) return;
     const int t0 = tile_start(i), tn = tile_len(i);
-    auto outside = [&](int nbid) { return nbid >= 0 && (unsigned)(nbid - t0) >= (unsigned)tn; };
-    for (int q = tid; q < tn * 16; q += kThreads) {
-      const int bl = q >> 4, k = q & 15;
+    for (int q = tid; q < tn * 4; q += kThreads) {
+      const int bl = q >> 2, f = q & 3;
       const int4 nb = sm.nbr[i % kStages][bl];
-      T(*h)[kBS] = sm.halo[i % kHaloSlots][bl];
-      const int f = k >> 3, r = k & 7;  // x face f, row r
-      const int nx = f == 0 ? nb.x : nb.y;
-      if (outside(nx)) cp_async<sizeof(T)>(&h[f][r], x + (size_t)nx * kBLEN + r * kBS + (f == 0 ? kBS - 1 : 0));
-      if (k < 2 * ROWC) {
-        const int g = k / ROWC, piece = k % ROWC;  // y face 2 + g
-        const int ny = g == 0 ? nb.z : nb.w;
-        if (outside(ny))
-          cp_async<16>(&h[2 + g][piece * (16 / (int)sizeof(T))],
-                       x + (size_t)ny * kBLEN + (g == 0 ? (kBS - 1) * kBS : 0) + piece * (16 / (int)sizeof(T)));
+      const int nbid = f == 0 ? nb.x : f == 1 ? nb.y : f == 2 ? nb.z : nb.w;
+      if (nbid < 0 || (unsigned)(nbid - t0) < (unsigned)tn) continue;
+      T* h = sm.halo[i % kHaloSlots][bl][f];
+      const T* src = x + (size_t)nbid * kBLEN;
+      if (f < 2) {
+        src += f == 0 ? kBS - 1 : 0;
+#pragma unroll
+        for (int r = 0; r < kBS; ++r) cp_async<sizeof(T)>(h + r, src + r * kBS);
+      } else {
+        src += f == 2 ? (kBS - 1) * kBS : 0;
+#pragma unroll
+        for (int piece = 0; piece < ROWC; ++piece)
+          cp_async<16>(h + piece * (16 / (int)sizeof(T)), src + piece * (16 / (int)sizeof(T)));
       }
     }
   };
@@ -216,28 +220,39 @@ __global__ void __launch_bounds__(kThreads) k_apply_staged(MeshView M, const T* 
     T* yt = y + (size_t)blk0 * kBLEN;
     for (int c = w; c < (n + CB - 1) / CB; c += kThreads / 32) {
       const int bl = c * CB + L.bl;
-      const bool valid = bl < n;
-      ChunkGather<T> g;
-      g.nb = valid ? sm.nbr[i % kStages][bl] : make_int4(kWall, kWall, kWall, kWall);
-      g.xm = g.xp = T(0);
-#pragma unroll
-      for (int j = 0; j < V; ++j) g.z[j] = g.ym[j] = g.yp[j] = T(0);
-      if (valid) {
-        const T(*h)[kBS] = sm.halo[i % kHaloSlots][bl];
-        auto in_tile = [&](int nbid) { return (unsigned)(nbid - blk0) < (unsigned)n; };
-        lds<V>(xs + bl * kBLEN + L.cell0, g.z);
-        if (L.ix0 == 0 && g.nb.x >= 0)
-          g.xm = in_tile(g.nb.x) ? xs[(g.nb.x - blk0) * kBLEN + L.iy * kBS + kBS - 1] : h[0][L.iy];
-        if (L.ix0 + V == kBS && g.nb.y >= 0)
-          g.xp = in_tile(g.nb.y) ? xs[(g.nb.y - blk0) * kBLEN + L.iy * kBS] : h[1][L.iy];
-        if (L.iy == 0 && g.nb.z >= 0)
-          lds<V>(in_tile(g.nb.z) ? xs + (g.nb.z - blk0) * kBLEN + (kBS - 1) * kBS + L.ix0 : &h[2][L.ix0], g.ym);
-        if (L.iy == kBS - 1 && g.nb.w >= 0)
-          lds<V>(in_tile(g.nb.w) ? xs + (g.nb.w - blk0) * kBLEN + L.ix0 : &h[3][L.ix0], g.yp);
-      }
+      if (bl >= n) continue;
+      const int4 nb = sm.nbr[i % kStages][bl];
+      const T(*h)[kBS] = sm.halo[i % kHaloSlots][bl];
+      const T* xb = xs + bl * kBLEN;
+      auto in_tile = [&](int nbid) { return (unsigned)(nbid - blk0) < (unsigned)n; };
+      T z[V], dn[V], up[V];
+      lds<V>(xb + L.cell0, z);
+      // neighbours: inside the block from shared memory, across a face from
+      // the same tile or the halo (address chosen, no branch), absent -> 0
+      const bool has_l = L.ix0 > 0 || nb.x >= 0, has_r = L.ix0 + V < kBS || nb.y >= 0;
+      const bool has_d = L.iy > 0 || nb.z >= 0, has_u = L.iy < kBS - 1 || nb.w >= 0;
+      const T* pl = L.ix0 > 0 ? xb + L.cell0 - 1
+                              : (in_tile(nb.x) ? xs + (nb.x - blk0) * kBLEN + L.iy * kBS + kBS - 1 : &h[0][L.iy]);
+      const T* pr = L.ix0 + V < kBS ? xb + L.cell0 + V
+                                    : (in_tile(nb.y) ? xs + (nb.y - blk0) * kBLEN + L.iy * kBS : &h[1][L.iy]);
+      const T* pd = L.iy > 0 ? xb + L.cell0 - kBS
+                             : (in_tile(nb.z) ? xs + (nb.z - blk0) * kBLEN + (kBS - 1) * kBS + L.ix0 : &h[2][L.ix0]);
+      const T* pu = L.iy < kBS - 1 ? xb + L.cell0 + kBS
+                                   : (in_tile(nb.w) ? xs + (nb.w - blk0) * kBLEN + L.ix0 : &h[3][L.ix0]);
+      const T vl = has_l ? *pl : T(0), vr = has_r ? *pr : T(0);
+      lds<V>(pd, dn);
+      lds<V>(pu, up);
       T out[V];
-      stencil_chunk<T>(g, L, out);
-      if (!valid) continue;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        T a = T(0);
+        int cnt = 0;
+        if (j > 0) { a += z[j - 1]; cnt++; } else if (has_l) { a += vl; cnt++; }
+        if (j < V - 1) { a += z[j + 1]; cnt++; } else if (has_r) { a += vr; cnt++; }
+        if (has_d) { a += dn[j]; cnt++; }
+        if (has_u) { a += up[j]; cnt++; }
+        out[j] = a - T(cnt) * z[j];
+      }
       const unsigned mk = (unsigned)(sm.mask[i % kStages][bl] >> L.cell0) & ((1u << V) - 1u);
       T* yo = yt + bl * kBLEN + L.cell0;
       if (mk == 0u) {
@@ -248,7 +263,8 @@ __global__ void __launch_bounds__(kThreads) k_apply_staged(MeshView M, const T* 
           if (!((mk >> j) & 1u)) yo[j] = out[j];
       }
     }
-    __syncthreads();  // the buffers of tile i are refilled from the next step on
+    // no barrier here: the next step's first barrier orders every read of
+    // tile i before its buffers are refilled
   }
   if (i < ntiles) {
     // a bulk copy did not complete in time: report, let the copies still in
