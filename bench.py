@@ -896,8 +896,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", choices=["batch", "large", "small", "serve", "timestep"], default="batch")
     ap.add_argument("--ts-steps", type=int, default=500, help="timestep workload: time steps per leg")
     ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
-    ap.add_argument("--team-mixed", type=int, default=16, help="batch: CTAs per problem, mixed")
-    ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64")
+    ap.add_argument("--team-mixed", type=int, default=8, help="batch: CTAs per problem, mixed (with --no-tune)")
+    ap.add_argument("--team-fp64", type=int, default=8, help="batch: CTAs per problem, FP64 (with --no-tune)")
     ap.add_argument("--no-tune", action="store_true", help="batch: fixed teams, no autotuner")
     ap.add_argument("--tune-iters", type=int, default=0,
                     help="batch autotuner: iterations per problem of a candidate (0 = full solves: a fixed "

@@ -2,9 +2,9 @@
 //
 // Stencil rows: the range passes (spmv_range) move 16 bytes per lane (see
 // Lane below); in-row and vertical neighbours come from warp shuffles, cells
-// across a same-level face from the neighbour block (or from another lane,
-// when that block is in the warp's span), and a wall face contributes no
-// flux.  Rows of cells on a coarse/fine face are skipped there.
+// across a same-level face from the neighbour block, and a wall face
+// contributes no flux.  Rows of cells on a coarse/fine face are skipped
+// there.
 //
 // Explicit rows (coarse/fine faces): stored as CSR, numbered contiguously by
 // block; every thread of the CTA takes rows of the CTA's row range.
@@ -30,6 +30,12 @@ __device__ __forceinline__ const float* row_vals<float>(const MeshView& M) { ret
 
 __device__ __forceinline__ int4 block_nbr(const MeshView& M, int blk) {
   return __ldg(reinterpret_cast<const int4*>(M.nbr) + blk);
+}
+
+template <class T>
+__device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, int blk, const int4& nb) {
+  if (nb.x == kExplicit || nb.y == kExplicit || nb.z == kExplicit || nb.w == kExplicit) return __ldg(M.xmask + blk);
+  return 0ull;
 }
 
 // ------------------------------------------------ 16-byte lane layout ----
@@ -104,13 +110,10 @@ struct ChunkGather {
   T ym[V], yp[V]; // across the y faces (rows 0 / 7)
 };
 
-// Loads of the lane's cells and of the halos across block faces; a face
-// whose neighbour is held by another lane of the warp (skip_*) is filled by
-// fill_siblings instead.
+// Loads of the lane's cells and of the halos across block faces.
 template <class T>
 __device__ __forceinline__ void gather_chunk(const int4& nb, int blk, bool valid, const T* __restrict__ z,
-                                             const Lane<T>& L, bool skip_xm, bool skip_xp, bool skip_ym,
-                                             bool skip_yp, ChunkGather<T>& g) {
+                                             const Lane<T>& L, ChunkGather<T>& g) {
   constexpr int V = Lane<T>::V;
   g.nb = nb;
   g.xm = g.xp = T(0);
@@ -118,10 +121,10 @@ __device__ __forceinline__ void gather_chunk(const int4& nb, int blk, bool valid
   for (int j = 0; j < V; ++j) g.z[j] = g.ym[j] = g.yp[j] = T(0);
   if (!valid) return;
   ldv<V>(z + blk * kBLEN + L.cell0, g.z);
-  if (L.ix0 == 0 && nb.x >= 0 && !skip_xm) g.xm = ldcg(z + nb.x * kBLEN + L.iy * kBS + (kBS - 1));
-  if (L.ix0 + V == kBS && nb.y >= 0 && !skip_xp) g.xp = ldcg(z + nb.y * kBLEN + L.iy * kBS);
-  if (L.iy == 0 && nb.z >= 0 && !skip_ym) ldv<V>(z + nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
-  if (L.iy == kBS - 1 && nb.w >= 0 && !skip_yp) ldv<V>(z + nb.w * kBLEN + L.ix0, g.yp);
+  if (L.ix0 == 0 && nb.x >= 0) g.xm = ldcg(z + nb.x * kBLEN + L.iy * kBS + (kBS - 1));
+  if (L.ix0 + V == kBS && nb.y >= 0) g.xp = ldcg(z + nb.y * kBLEN + L.iy * kBS);
+  if (L.iy == 0 && nb.z >= 0) ldv<V>(z + nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, g.ym);
+  if (L.iy == kBS - 1 && nb.w >= 0) ldv<V>(z + nb.w * kBLEN + L.ix0, g.yp);
 }
 
 // Stencil rows of the lane's cells, summed left, right, below, above as the
@@ -157,81 +160,15 @@ __device__ __forceinline__ void stencil_chunk(const ChunkGather<T>& g, const Lan
   }
 }
 
-// Which faces of the lane's block in a span are shared with another block
-// of the same span (Morton siblings: the next block in x, two blocks on in
-// y for FP32 spans of four blocks).
-struct Siblings {
-  bool xm, xp, ym, yp;
-};
-
-// A warp's span: 2*CB consecutive blocks, chunk a = the first CB, chunk b =
-// the next CB.  FP32 (CB = 2): in each chunk the lower half-warp's block and
-// the upper half-warp's block are consecutive, and chunk b's blocks are two
-// on from chunk a's.  FP64 (CB = 1): chunk b's block follows chunk a's.
-template <class T>
-__device__ __forceinline__ void span_siblings(const int4& na, const int4& nbb, int ba, int bb, int b1,
-                                              const Lane<T>& L, Siblings& sa, Siblings& sb) {
-  if constexpr (Lane<T>::CB == 2) {
-    // chunk-internal x faces (bl 0 <-> bl 1), y faces across the chunks
-    sa.xp = L.bl == 0 && na.y == ba + 1 && ba + 1 < b1;
-    sa.xm = L.bl == 1 && na.x == ba - 1;
-    sa.yp = na.w == ba + 2 && ba + 2 < b1;
-    sa.ym = false;
-    sb.xp = L.bl == 0 && nbb.y == bb + 1 && bb + 1 < b1;
-    sb.xm = L.bl == 1 && nbb.x == bb - 1;
-    sb.yp = false;
-    sb.ym = nbb.z == bb - 2 && bb < b1;
-  } else {
-    sa.xp = na.y == ba + 1 && ba + 1 < b1;
-    sa.xm = sa.ym = sa.yp = false;
-    sb.xm = nbb.x == bb - 1 && bb < b1;
-    sb.xp = sb.ym = sb.yp = false;
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void fill_siblings(ChunkGather<T>& ga, ChunkGather<T>& gb, const Siblings& sa,
-                                              const Siblings& sb, const Lane<T>& L, int lane) {
-  constexpr int V = Lane<T>::V;
-  if constexpr (Lane<T>::CB == 2) {
-    // x: block bl 0's right edge <- bl 1's column 0 (lane + 15), bl 1's left
-    // edge <- bl 0's column 7 (lane - 15)
-    const T an = __shfl_sync(kFull, ga.z[0], (lane + 15) & 31), ap = __shfl_sync(kFull, ga.z[V - 1], (lane - 15) & 31);
-    const T bn = __shfl_sync(kFull, gb.z[0], (lane + 15) & 31), bp = __shfl_sync(kFull, gb.z[V - 1], (lane - 15) & 31);
-    if (sa.xp) ga.xp = an;
-    if (sa.xm) ga.xm = ap;
-    if (sb.xp) gb.xp = bn;
-    if (sb.xm) gb.xm = bp;
-    // y: chunk a's row 7 <- chunk b's row 0 (lane - 14), chunk b's row 0 <-
-    // chunk a's row 7 (lane + 14)
-#pragma unroll
-    for (int j = 0; j < V; ++j) {
-      const T u = __shfl_sync(kFull, gb.z[j], (lane - 14) & 31);
-      const T d = __shfl_sync(kFull, ga.z[j], (lane + 14) & 31);
-      if (sa.yp) ga.yp[j] = u;
-      if (sb.ym) gb.ym[j] = d;
-    }
-  } else {
-    // x: chunk a's right edge <- chunk b's column 0 (lane - 3), chunk b's
-    // left edge <- chunk a's column 7 (lane + 3)
-    const T n = __shfl_sync(kFull, gb.z[0], (lane - 3) & 31);
-    const T p = __shfl_sync(kFull, ga.z[V - 1], (lane + 3) & 31);
-    if (sa.xp) ga.xp = n;
-    if (sb.xm) gb.xm = p;
-  }
-  (void)L;
-}
-
-// xmask: the block's explicit-row mask (fetched with its neighbour table).
 template <class T, class Epi>
-__device__ __forceinline__ void chunk_epilogue(const ChunkGather<T>& g, const Lane<T>& L, int blk, bool valid,
-                                               unsigned long long xmask, const typename Epi::Pre& pre, Epi& epi) {
+__device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGather<T>& g, const Lane<T>& L,
+                                               int blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
   constexpr int V = Lane<T>::V;
   T y[V];
   stencil_chunk<T>(g, L, y);
   if (!valid) return;
   const int i0 = blk * kBLEN + L.cell0;
-  const unsigned mk = (unsigned)(xmask >> L.cell0) & ((1u << V) - 1u);
+  const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, g.nb) >> L.cell0) & ((1u << V) - 1u);
   if (mk == 0u) {
     epi.vec(i0, y, pre);
   } else {
@@ -251,16 +188,18 @@ __device__ __forceinline__ void chunk_epilogue(const ChunkGather<T>& g, const La
 //   one(i, y, pre, j)            cell i, element j of pre (lanes owning an
 //                                explicit row, and the explicit rows);
 // each cell of the ranges is handed over exactly once, by one thread, in no
-// particular order.  A warp takes spans of 2*CB consecutive blocks (two
-// chunks in flight), takes the halos of sibling blocks inside the span from
-// shuffles, and fetches the neighbour tables and explicit-row masks of its
-// next span while it computes the current one.  The explicit rows' offsets
+// particular order.  A warp takes one chunk (CB consecutive blocks) per step
+// and fetches the neighbour table of its next chunk while it computes the
+// current one; the halos across block faces are loaded from the neighbours
+// (one chunk in flight per warp keeps the solver kernels' register state
+// small: two chunks with halos shuffled between Morton siblings spilled more
+// and measured 10 % slower on the mixed batch).  The explicit rows' offsets
 // are fetched before the stencil loop.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int b0, int b1,
                                            int r0, int r1, Epi& epi) {
   using Pre = typename Epi::Pre;
-  constexpr int CB = Lane<T>::CB, SPAN = 2 * CB;
+  constexpr int CB = Lane<T>::CB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const Lane<T> L(lane);
   // explicit rows: this thread's first row, its offsets and cell, early
@@ -272,34 +211,21 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
     k1 = __ldg(M.xptr + r + 1);
     cell = __ldg(M.rowcell + r);
   }
-  const int nsp = (b1 - b0 + SPAN - 1) / SPAN;
+  const int nch = (b1 - b0 + CB - 1) / CB;
   auto nbr_of = [&](int blk) {
     return blk < b1 ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
   };
-  auto mask_of = [&](int blk) { return blk < b1 ? __ldg(M.xmask + blk) : 0ull; };
-  int sp = w;
-  int4 na = nbr_of(b0 + sp * SPAN + L.bl), nbb = nbr_of(b0 + sp * SPAN + CB + L.bl);
-  unsigned long long ma = mask_of(b0 + sp * SPAN + L.bl), mb = mask_of(b0 + sp * SPAN + CB + L.bl);
-  for (; sp < nsp; sp += nw) {
-    const int ba = b0 + sp * SPAN + L.bl, bb = ba + CB;
-    const bool va = ba < b1, vb = bb < b1;
-    Siblings sa, sb;
-    span_siblings<T>(na, nbb, ba, bb, b1, L, sa, sb);
-    ChunkGather<T> ga, gb;
-    gather_chunk<T>(na, ba, va, z, L, sa.xm, sa.xp, sa.ym, sa.yp, ga);
-    gather_chunk<T>(nbb, bb, vb, z, L, sb.xm, sb.xp, sb.ym, sb.yp, gb);
-    Pre pa{}, pb{};
+  int ch = w;
+  int4 na = nbr_of(b0 + ch * CB + L.bl);
+  for (; ch < nch; ch += nw) {
+    const int ba = b0 + ch * CB + L.bl;
+    const bool va = ba < b1;
+    ChunkGather<T> ga;
+    gather_chunk<T>(na, ba, va, z, L, ga);
+    Pre pa{};
     if (va) pa = epi.load(ba * kBLEN + L.cell0);
-    if (vb) pb = epi.load(bb * kBLEN + L.cell0);
-    const unsigned long long cma = ma, cmb = mb;
-    const int nxt = b0 + (sp + nw) * SPAN + L.bl;
-    na = nbr_of(nxt);
-    nbb = nbr_of(nxt + CB);
-    ma = mask_of(nxt);
-    mb = mask_of(nxt + CB);
-    fill_siblings<T>(ga, gb, sa, sb, L, lane);
-    chunk_epilogue<T>(ga, L, ba, va, cma, pa, epi);
-    chunk_epilogue<T>(gb, L, bb, vb, cmb, pb, epi);
+    na = nbr_of(b0 + (ch + nw) * CB + L.bl);
+    chunk_epilogue<T>(M, ga, L, ba, va, pa, epi);
   }
   for (; r < r1; r += blockDim.x) {
     const Pre pre = epi.load1(cell);
