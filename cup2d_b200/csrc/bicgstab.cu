@@ -91,6 +91,16 @@ struct Smem {
   int slot;           // batch: the problem the team works on
 };
 
+// the warp's block row of the staging tile, as SpMV scratch
+template <class T>
+__device__ __forceinline__ T* spmv_row(Smem& sm);
+template <>
+__device__ __forceinline__ double* spmv_row<double>(Smem& sm) { return sm.tile.d[0][threadIdx.x >> 5]; }
+template <>
+__device__ __forceinline__ float* spmv_row<float>(Smem& sm) {
+  return sm.tile.f[0][2 * (threadIdx.x >> 5) + ((threadIdx.x & 31) >> 4)];
+}
+
 // max that propagates NaN (fmax drops it, which would let a blown-up
 // residual read as converged)
 __device__ __forceinline__ double nanmax(double a, double b) { return (a > b || a != a) ? a : b; }
@@ -384,7 +394,7 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       if (set_rh) rh[i] = r32;
     }
   } epi{b, mean_b, r, rh, set_rh, {0.0, 0.0, 0.0, 0.0, 0.0}};
-  spmv_range<double>(M, x, b0, b1, r0, r1, epi);
+  spmv_range<double>(M, x, b0, b1, r0, r1, epi, spmv_row<double>(sm));
   cta_partials<5>(sm, epi.v, 0x11u, red, Q_RU);
 }
 
@@ -480,7 +490,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, cons
     // pass B: nu = A z; (rhat, nu)
     {
       EpiRhNu<T> epi{V.rh, V.nu, 0.0};
-      spmv_range<T>(M, V.z, b0, b1, r0, r1, epi);
+      spmv_range<T>(M, V.z, b0, b1, r0, r1, epi, spmv_row<T>(sm));
       const double v[1] = {epi.acc};
       cta_partials<1>(sm, v, 0u, red, Q_RHNU);
     }
@@ -526,7 +536,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, cons
     // pass D: t = A z2; (t,s), (t,t)
     {
       EpiTS<T> epi{V.r, V.t, 0.0, 0.0};
-      spmv_range<T>(M, V.z2, b0, b1, r0, r1, epi);
+      spmv_range<T>(M, V.z2, b0, b1, r0, r1, epi, spmv_row<T>(sm));
       const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
     }
@@ -738,7 +748,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
         rh[i] = rv;
       }
     } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
-    spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi);
+    spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi, spmv_row<double>(sm));
     cta_partials<3>(sm, epi.v, 0x3u, red, Q_INIT);
   }
   if (!B.sync(&sm.flag, 0)) return false;

@@ -1,10 +1,10 @@
 // Block-structured SpMV: y = A z over a range of 8x8 blocks.
 //
 // Stencil rows: the range passes (spmv_range) move 16 bytes per lane (see
-// Lane below); in-row and vertical neighbours come from warp shuffles, cells
-// across a same-level face from the neighbour block, and a wall face
-// contributes no flux.  Rows of cells on a coarse/fine face are skipped
-// there.
+// Lane below); in-row and vertical neighbours come from the warp's block row
+// in shared memory, cells across a same-level face from the neighbour
+// block, and a wall face contributes no flux.  Rows of cells on a
+// coarse/fine face are skipped there.
 //
 // Explicit rows (coarse/fine faces): stored as CSR, numbered contiguously by
 // block; every thread of the CTA takes rows of the CTA's row range.
@@ -128,44 +128,60 @@ __device__ __forceinline__ void gather_chunk(const int4& nb, int blk, bool valid
 }
 
 // Stencil rows of the lane's cells, summed left, right, below, above as the
-// assembled rows are (explicit rows get meaningless values).  All lanes of
-// the warp take part (shuffles).
+// assembled rows are (explicit rows get meaningless values).  The warp
+// writes its chunk to its block row in shared memory (`row`: kBLEN values,
+// 16-byte aligned) and reads the in-block neighbours back from there (a
+// lane's row above and below as whole vectors); cells across a block face
+// come from the halo loads.  All lanes of the warp take part.  Shuffling the
+// neighbours instead took more instructions (two per FP64 value) and kept
+// more registers live: measured 8 % slower on the mixed batch.
 template <class T>
-__device__ __forceinline__ void stencil_chunk(const ChunkGather<T>& g, const Lane<T>& L, T (&y)[Lane<T>::V]) {
-  constexpr int V = Lane<T>::V, LR = Lane<T>::LR;
-  const T from_l = __shfl_up_sync(kFull, g.z[V - 1], 1);
-  const T from_r = __shfl_down_sync(kFull, g.z[0], 1);
+__device__ __forceinline__ void stencil_chunk_smem(const ChunkGather<T>& g, const Lane<T>& L, T* row,
+                                                   T (&y)[Lane<T>::V]) {
+  constexpr int V = Lane<T>::V;
+  stv<V>(row + L.cell0, g.z);
+  __syncwarp();
+  const bool has_l = L.ix0 > 0 || g.nb.x >= 0, has_r = L.ix0 + V < kBS || g.nb.y >= 0;
+  const bool has_d = L.iy > 0 || g.nb.z >= 0, has_u = L.iy < kBS - 1 || g.nb.w >= 0;
+  const T vl = L.ix0 > 0 ? row[L.cell0 - 1] : g.xm;
+  const T vr = L.ix0 + V < kBS ? row[L.cell0 + V] : g.xp;
   T dn[V], up[V];
+  if (L.iy > 0) {
+    const T* p = row + L.cell0 - kBS;
 #pragma unroll
-  for (int j = 0; j < V; ++j) {
-    dn[j] = __shfl_up_sync(kFull, g.z[j], LR);
-    up[j] = __shfl_down_sync(kFull, g.z[j], LR);
+    for (int j = 0; j < V; ++j) dn[j] = p[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) dn[j] = g.ym[j];
   }
-  const bool left_in = (L.sub % LR) > 0, right_in = (L.sub % LR) < LR - 1;
+  if (L.iy < kBS - 1) {
+    const T* p = row + L.cell0 + kBS;
+#pragma unroll
+    for (int j = 0; j < V; ++j) up[j] = p[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) up[j] = g.yp[j];
+  }
+  __syncwarp();
 #pragma unroll
   for (int j = 0; j < V; ++j) {
     T a = T(0);
     int n = 0;
-    if (j > 0) { a += g.z[j - 1]; n++; }
-    else if (left_in) { a += from_l; n++; }
-    else if (g.nb.x >= 0) { a += g.xm; n++; }
-    if (j < V - 1) { a += g.z[j + 1]; n++; }
-    else if (right_in) { a += from_r; n++; }
-    else if (g.nb.y >= 0) { a += g.xp; n++; }
-    if (L.iy > 0) { a += dn[j]; n++; }
-    else if (g.nb.z >= 0) { a += g.ym[j]; n++; }
-    if (L.iy < kBS - 1) { a += up[j]; n++; }
-    else if (g.nb.w >= 0) { a += g.yp[j]; n++; }
+    if (j > 0) { a += g.z[j - 1]; n++; } else if (has_l) { a += vl; n++; }
+    if (j < V - 1) { a += g.z[j + 1]; n++; } else if (has_r) { a += vr; n++; }
+    if (has_d) { a += dn[j]; n++; }
+    if (has_u) { a += up[j]; n++; }
     y[j] = a - T(n) * g.z[j];
   }
 }
 
 template <class T, class Epi>
 __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGather<T>& g, const Lane<T>& L,
-                                               int blk, bool valid, const typename Epi::Pre& pre, Epi& epi) {
+                                               int blk, bool valid, const typename Epi::Pre& pre, Epi& epi,
+                                               T* row) {
   constexpr int V = Lane<T>::V;
   T y[V];
-  stencil_chunk<T>(g, L, y);
+  stencil_chunk_smem<T>(g, L, row, y);
   if (!valid) return;
   const int i0 = blk * kBLEN + L.cell0;
   const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, g.nb) >> L.cell0) & ((1u << V) - 1u);
@@ -179,7 +195,8 @@ __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGat
 }
 
 // y = A z: the stencil rows of blocks [b0, b1) and the explicit rows
-// [r0, r1), by the whole CTA, in the 16-byte layout.  The epilogue functor
+// [r0, r1), by the whole CTA, in the 16-byte layout; `row` is the lane's
+// block row of the warp's shared-memory scratch.  The epilogue functor
 // provides
 //   Pre load(i0) / Pre load1(i)  operands of the lane's V cells from i0 (or
 //                                of one cell i, as element 0), loaded with
@@ -197,7 +214,7 @@ __device__ __forceinline__ void chunk_epilogue(const MeshView& M, const ChunkGat
 // are fetched before the stencil loop.
 template <class T, class Epi>
 __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restrict__ z, int b0, int b1,
-                                           int r0, int r1, Epi& epi) {
+                                           int r0, int r1, Epi& epi, T* row) {
   using Pre = typename Epi::Pre;
   constexpr int CB = Lane<T>::CB;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -225,7 +242,7 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
     Pre pa{};
     if (va) pa = epi.load(ba * kBLEN + L.cell0);
     na = nbr_of(b0 + (ch + nw) * CB + L.bl);
-    chunk_epilogue<T>(M, ga, L, ba, va, pa, epi);
+    chunk_epilogue<T>(M, ga, L, ba, va, pa, epi, row);
   }
   for (; r < r1; r += blockDim.x) {
     const Pre pre = epi.load1(cell);
