@@ -32,3 +32,16 @@ def test_adapter_solves(tmp_path, cuda):
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "status 0" in r.stdout
+
+
+def test_c_batch_caller_compiles_as_c(tmp_path, has_gpu):
+    """The header compiles as strict C11 with the batch, graph and
+    time-stepping declarations; without a device the batch reports it."""
+    exe = tmp_path / "batch_demo"
+    subprocess.run(["gcc", "-std=c11", "-O1", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "cpp" / "batch_demo.c"), "-L", str(L.LIB_PATH.parent),
+                    "-lcup2d_poisson", f"-Wl,-rpath,{L.LIB_PATH.parent}", "-o", str(exe)], check=True)
+    if has_gpu:
+        pytest.skip("a GPU is present: the batch path is covered by the gpu-marked batch tests")
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 2, r.stdout + r.stderr
