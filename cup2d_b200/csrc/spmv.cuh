@@ -45,7 +45,8 @@ __device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, i
 // for FP64 (a warp covers one block).  A "chunk" is the CB blocks one warp
 // access covers.  Lane l of a chunk owns cells cell0 .. cell0 + V - 1 of
 // block bl, row iy; in-row neighbours of other lanes and the rows above and
-// below come from shuffles, cells across a block face from the neighbour.
+// below come from the warp's block row in shared memory, cells across a
+// block face from the neighbour block.
 
 template <class T>
 struct Lane {
