@@ -108,11 +108,14 @@ def _dist():
 
 
 def _max_over_ranks(v: float, world: int) -> float:
+    """The largest of the ranks' values (times are max over ranks): one
+    scalar all-reduce, on the device for NCCL, on the host for gloo."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
