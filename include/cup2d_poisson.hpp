@@ -14,8 +14,10 @@
 // std::runtime_error carrying the status string; nothing exits.
 #pragma once
 
+#include <algorithm>
 #include <memory>
 #include <stdexcept>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -93,6 +95,57 @@ class ExpAMRSolver : public PoissonSolver {
   SimulationData& sim_;
   cup2d_poisson* h_ = nullptr;
   cup2d_solve_stats last_{};
+};
+
+// Many independent problems in one persistent launch (cup2d_batch_*): each
+// problem gets exactly the solve above.  Host-buffer solves, device-pointer
+// solves, the launch-shape autotuner and CUDA-graph replay.
+class BatchSolver {
+ public:
+  BatchSolver(const std::vector<cup2d_forest>& forests, const cup2d_solve_opts& opts) {
+    check(cup2d_batch_create((int32_t)forests.size(), forests.data(), &opts, &b_), "cup2d_batch_create");
+  }
+  ~BatchSolver() { cup2d_batch_destroy(b_); }
+  BatchSolver(const BatchSolver&) = delete;
+  BatchSolver& operator=(const BatchSolver&) = delete;
+
+  int32_t size() const { return cup2d_batch_size(b_); }
+  // host buffers: b[i] the RHS, x[i] initial guess in, solution out
+  std::vector<cup2d_solve_stats> solve(const std::vector<const double*>& b, const std::vector<double*>& x) {
+    std::vector<cup2d_solve_stats> st((size_t)size());
+    check(cup2d_batch_solve(b_, b.data(), x.data(), st.data()), "cup2d_batch_solve");
+    return st;
+  }
+  // device pointers, on `stream` (a cudaStream_t)
+  std::vector<cup2d_solve_stats> solve_device(const std::vector<const double*>& d_b,
+                                              const std::vector<double*>& d_x, void* stream = nullptr) {
+    std::vector<cup2d_solve_stats> st((size_t)size());
+    check(cup2d_batch_solve_device(b_, d_b.data(), d_x.data(), st.data(), stream), "cup2d_batch_solve_device");
+    return st;
+  }
+  // the fastest (team, CTAs per SM) among the candidates, kept for later solves
+  std::pair<int32_t, int32_t> tune(const std::vector<const double*>& d_b, const std::vector<double*>& d_x,
+                                   const std::vector<int32_t>& teams, const std::vector<int32_t>& ctas_per_sm,
+                                   int32_t iters = 0) {
+    std::vector<double> rates(teams.size() * std::max<size_t>(1, ctas_per_sm.size()));
+    int32_t team = 0, cps = 0;
+    check(cup2d_batch_tune(b_, d_b.data(), d_x.data(), teams.data(), (int32_t)teams.size(), ctas_per_sm.data(),
+                           (int32_t)ctas_per_sm.size(), iters, rates.data(), &team, &cps),
+          "cup2d_batch_tune");
+    return {team, cps};
+  }
+  void capture(const std::vector<const double*>& d_b, const std::vector<double*>& d_x, bool zero_x = false) {
+    check(cup2d_batch_capture(b_, d_b.data(), d_x.data(), zero_x ? CUP2D_GRAPH_ZERO_X : 0), "cup2d_batch_capture");
+  }
+  void replay(void* stream = nullptr) { check(cup2d_batch_replay(b_, stream), "cup2d_batch_replay"); }
+  std::vector<cup2d_solve_stats> replay_stats() {
+    std::vector<cup2d_solve_stats> st((size_t)size());
+    check(cup2d_batch_replay_stats(b_, st.data()), "cup2d_batch_replay_stats");
+    return st;
+  }
+
+ private:
+  cup2d_batch* b_ = nullptr;
 };
 
 inline std::shared_ptr<PoissonSolver> makePoissonSolver(SimulationData& s, const cup2d_forest& forest) {

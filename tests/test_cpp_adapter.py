@@ -45,3 +45,16 @@ def test_c_batch_caller_compiles_as_c(tmp_path, has_gpu):
         pytest.skip("a GPU is present: the batch path is covered by the gpu-marked batch tests")
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 2, r.stdout + r.stderr
+
+
+def test_cpp_batch_wrapper_compiles(tmp_path, has_gpu):
+    """The C++ batch wrapper (cup2d_poisson.hpp) compiles with -Wall -Werror
+    and, without a device, reports it through its exception."""
+    exe = tmp_path / "batch_cpp_demo"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "cpp" / "batch_cpp_demo.cpp"), "-L", str(L.LIB_PATH.parent),
+                    "-lcup2d_poisson", f"-Wl,-rpath,{L.LIB_PATH.parent}", "-o", str(exe)], check=True)
+    if has_gpu:
+        pytest.skip("a GPU is present: the batch path is covered by the gpu-marked batch tests")
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 2 and "no CUDA device" in r.stdout, r.stdout + r.stderr
