@@ -213,6 +213,15 @@ class Solver:
         return r.value, z.value
 
 
+def tune_key(device_name: str, precision: int, nblocks, teams, ctas_per_sm) -> str:
+    """Cache key of an autotuner choice: the GPU, the precision, the batch
+    size, its size quantiles (10/50/90/100 %) and the candidate lists."""
+    sizes = np.sort(np.asarray(nblocks, dtype=np.int64))
+    q = ",".join(str(int(sizes[int(f * (len(sizes) - 1))])) for f in (0.1, 0.5, 0.9, 1.0))
+    return "|".join([device_name, "mixed" if precision == L.PREC_MIXED else "fp64", f"n={len(sizes)}", "q=" + q,
+                     "teams=" + ",".join(map(str, teams)), "cps=" + ",".join(map(str, ctas_per_sm))])
+
+
 class BatchSolver:
     """Many independent problems in one persistent launch (no counterpart in
     the reference, which solves one problem per PoissonSolver::solve call;
@@ -297,11 +306,8 @@ class BatchSolver:
         import os
 
         import torch
-        sizes = np.sort([self.ncells(i) // 64 for i in range(len(self))])
-        key = "|".join([torch.cuda.get_device_name(), "mixed" if self.opts.precision == L.PREC_MIXED else "fp64",
-                        f"n={len(sizes)}", "q=" + ",".join(str(int(sizes[int(q * (len(sizes) - 1))]))
-                                                              for q in (0.1, 0.5, 0.9, 1.0)),
-                        "teams=" + ",".join(map(str, teams)), "cps=" + ",".join(map(str, ctas_per_sm))])
+        key = tune_key(torch.cuda.get_device_name(), self.opts.precision,
+                       [self.ncells(i) // 64 for i in range(len(self))], teams, ctas_per_sm)
         table = {}
         if cache and os.path.exists(cache):
             with open(cache) as f:
