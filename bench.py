@@ -317,7 +317,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         "clocks": clk.summary(),
         "status_ok": all(s["status"] == 0 for s in st_mixed + st_fp64),
     }
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:  # the host baseline: rank 0 at N=1 only
         line["cpu_baseline"] = cpu_baseline(mesh, bs[args.warmup].cpu().numpy(), statistics.mean(it_d))
     return line
 
@@ -544,7 +544,7 @@ def run_batch(args, world, rank, local) -> dict | None:
     }
     if not args.no_serve:
         line["serving"] = run_serve(args)
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:  # the host baseline: rank 0 at N=1 only
         idx = batch_sample(meshes)
         sec, tot, cores = oracle_cell_iter_seconds(meshes, seeds, idx, args.cpu_iters)
         per_solve = sec * cit_64 / n
