@@ -11,12 +11,9 @@ from cup2d_b200 import Cup2dError, Mesh, Solver
 from cup2d_b200 import _lib as L
 from cup2d_b200.mesh import fourier_advance, fourier_coefs
 from cup2d_b200.problems import EXTENT, sized_mesh, small_mesh
+from transfer_rule import disk_mesh as _disk_mesh, transfer_restated as _transfer_restated
 
 pytestmark = pytest.mark.gpu
-
-
-def _disk_mesh(shift: float, level_max: int = 5, band: float = 0.1) -> Mesh:
-    return Mesh.disks(8, 4, level_max, EXTENT, [(0.6 + shift, 0.5, 0.1), (1.3 - shift, 0.4, 0.07)], band)
 
 
 def _meshes():
@@ -42,42 +39,6 @@ def test_rhs_device_matches_host(cuda, name):
     assert np.max(np.abs(bd - b_host)) <= 1e-12 * scale
     assert abs(float(np.sum(bd))) <= 1e-12 * float(np.sum(np.abs(bd)))
     assert np.array_equal(m.rhs_fourier(17), m.rhs_from_coefs(fourier_coefs(17)))
-
-
-def _transfer_restated(src: Mesh, xs: np.ndarray, dst: Mesh) -> np.ndarray:
-    """Restatement of the transfer rule: positions in cells of level G =
-    max(levelMax) + 1; same-level or finer dst cells take the src cell
-    holding their centre, coarser ones the mean of the src cells at their
-    quadrant centres."""
-    G = max(src.level_max, dst.level_max) + 1
-    leaf = {(int(l), int(i), int(j)): k for k, (l, i, j) in enumerate(zip(src.level, src.bx, src.by))}
-
-    def locate(px, py):
-        for l in range(src.level_max):
-            ci, cj = px >> (G - l), py >> (G - l)
-            k = leaf.get((l, ci >> 3, cj >> 3))
-            if k is not None:
-                return k, (cj & 7) * 8 + (ci & 7)
-        raise AssertionError("point outside the forest")
-
-    out = np.empty(dst.ncells)
-    for b, (l, bi, bj) in enumerate(zip(dst.level, dst.bx, dst.by)):
-        sh = G - int(l)
-        for c in range(64):
-            ix, iy = c & 7, c >> 3
-            px = ((int(bi) * 8 + ix) << sh) + (1 << (sh - 1))
-            py = ((int(bj) * 8 + iy) << sh) + (1 << (sh - 1))
-            k, sc = locate(px, py)
-            if src.level[k] <= l:
-                out[b * 64 + c] = xs[k * 64 + sc]
-                continue
-            q = 1 << (sh - 2)
-            acc = 0.0
-            for t in range(4):
-                k2, c2 = locate(px + (q if t & 1 else -q), py + (q if t & 2 else -q))
-                acc += xs[k2 * 64 + c2]
-            out[b * 64 + c] = 0.25 * acc
-    return out
 
 
 @pytest.mark.parametrize("shift,lmax", [(0.0, 5), (0.05, 5), (0.12, 5), (0.05, 4), (0.05, 6)])
