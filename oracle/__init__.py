@@ -1,4 +1,4 @@
-"""ORACLE — test infrastructure only (parity checker and timed CPU baseline).
+"""ORACLE — test infrastructure only (reference for the parity tests and timed CPU baseline).
 
 ctypes binding of oracle/liboracle.so, the CPU FP64 restatement of CUP2D's
 GPU Poisson path (see oracle.cpp for the reference lines it follows).  Only

@@ -1,5 +1,5 @@
 // ORACLE — test infrastructure only.  CPU FP64 restatement of CUP2D's GPU
-// Poisson path, used as the parity checker and as the timed CPU baseline.
+// Poisson path, used as the reference of the parity tests and as the timed CPU baseline.
 // Nothing in the product library links, loads or calls this file.
 //
 // What it restates (paths relative to the CUP2D source tree):

@@ -1,6 +1,6 @@
-"""Properties of the restated transfer rule (the checker of the device
-kernel), on the CPU: identity on the same forest, constants preserved,
-every value a copy or a convex mean of source values."""
+"""Properties of the restated transfer rule (what the device kernel is
+compared with), on the CPU: identity on the same forest, constants
+preserved, every value a copy or a convex mean of source values."""
 import numpy as np
 
 from transfer_rule import disk_mesh, transfer_restated
