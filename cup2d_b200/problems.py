@@ -27,6 +27,13 @@ def small_mesh() -> Mesh:
     return Mesh.disks(4, 2, 4, EXTENT, [(0.6, 0.5, 0.1)], 0.15)
 
 
+def quoted_small_mesh() -> Mesh:
+    """The small configuration at its quoted size (~300 blocks, ~19k cells):
+    the same domain, level count and disk with the refinement band widened
+    to 0.43, which gives 302 blocks / 19,328 cells (band 0.15 gives 128)."""
+    return Mesh.disks(4, 2, 4, EXTENT, [(0.6, 0.5, 0.1)], 0.43)
+
+
 def seeded_disks(rng: np.random.Generator, count: int, rmin: float = 0.05, rmax: float = 0.1):
     return [(float(rng.uniform(0.3, 1.7)), float(rng.uniform(0.25, 0.75)), float(rng.uniform(rmin, rmax)))
             for _ in range(count)]

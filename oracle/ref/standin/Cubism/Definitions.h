@@ -1,0 +1,3 @@
+// Stand-in for Cubism/Definitions.h: the whole stand-in lives in cubism_standin.hpp.
+#pragma once
+#include "../cubism_standin.hpp"

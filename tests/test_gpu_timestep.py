@@ -11,7 +11,7 @@ from cup2d_b200 import Cup2dError, Mesh, Solver
 from cup2d_b200 import _lib as L
 from cup2d_b200.mesh import fourier_advance, fourier_coefs
 from cup2d_b200.problems import EXTENT, sized_mesh, small_mesh
-from transfer_rule import disk_mesh as _disk_mesh, transfer_restated as _transfer_restated
+from tests.transfer_rule import disk_mesh as _disk_mesh, transfer_restated as _transfer_restated
 
 pytestmark = pytest.mark.gpu
 

@@ -3,7 +3,7 @@ compared with), on the CPU: identity on the same forest, constants
 preserved, every value a copy or a convex mean of source values."""
 import numpy as np
 
-from transfer_rule import disk_mesh, transfer_restated
+from tests.transfer_rule import disk_mesh, transfer_restated
 
 
 def test_identity_and_constants():
