@@ -45,6 +45,7 @@
 // only on the true FP64 residual.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
@@ -70,18 +71,45 @@ enum : int {
 };
 static_assert(Q_SUMB + 1 <= kRedQ, "reduction slots");
 
-// P^-1 operand in shared memory: FP64 rows, or the TF32 split (hi, lo)
-union PinvSmem {
-  double d[kBLEN][kPad];
-  uint32_t f[2][kBLEN][kPad];
+// Shared memory of the solve kernels, per precision T of the Krylov vectors:
+// P^-1, the P^-1 staging tiles, the staged SpMV rings and the reduction
+// scratch.  Both layouts stay below 54 KB so that three CTAs per SM fit the
+// 164 KB shared carve-out and leave 92 KB of the unified L1/shared array as
+// L1 (the kernels' spill reloads and table reads live there: the same
+// kernel with the whole array given to shared memory ran 11 % slower).
+template <class T>
+union TileSmem;
+template <>
+union TileSmem<double> {
+  double d[2][8][kPad];             // P^-1 staging tiles, FP64 SpMV scratch
+  SpmvStage<double> s64[kWarps];    // staged SpMV rings (passes B, D), one per warp
+};
+template <>
+union TileSmem<float> {
+  double d[2][8][kPad];             // FP64 SpMV scratch (true residual)
+  float f[2][16][kPad];             // P^-1 staging tiles
+  SpmvStage<float> s32[kWarps];     // staged SpMV rings (passes B, D), one per warp
 };
 
+// P^-1 operand: FP64 rows, or the TF32 split of the FP32 P^-1 (hi, lo),
+// in rows of 64 values with the columns XOR-swizzled by the row (see the
+// Pinv specialisations): conflict-free fragment loads without padding.
+template <class T>
+struct PinvSmem;
+template <>
+struct PinvSmem<double> {
+  double v[kBLEN][kBLEN];
+};
+template <>
+struct PinvSmem<float> {
+  uint32_t hi[kBLEN][kBLEN];
+  uint32_t lo[kBLEN][kBLEN];
+};
+
+template <class T>
 struct Smem {
-  PinvSmem P;
-  union {
-    double d[2][8][kPad];
-    float f[2][16][kPad];
-  } tile;
+  PinvSmem<T> P;
+  TileSmem<T> tile;
   double wred[kWarps][6];
   double gres[6];
   int flag;
@@ -91,22 +119,22 @@ struct Smem {
   int slot;           // batch: the problem the team works on
 };
 
-// the warp's block row of the staging tile, as SpMV scratch
-template <class T>
-__device__ __forceinline__ T* spmv_row(Smem& sm);
-template <>
-__device__ __forceinline__ double* spmv_row<double>(Smem& sm) { return sm.tile.d[0][threadIdx.x >> 5]; }
-template <>
-__device__ __forceinline__ float* spmv_row<float>(Smem& sm) {
-  return sm.tile.f[0][2 * (threadIdx.x >> 5) + ((threadIdx.x & 31) >> 4)];
+// the warp's ring of the staged SpMV
+__device__ __forceinline__ SpmvStage<float>& spmv_stage(Smem<float>& sm) { return sm.tile.s32[threadIdx.x >> 5]; }
+__device__ __forceinline__ SpmvStage<double>& spmv_stage(Smem<double>& sm) { return sm.tile.s64[threadIdx.x >> 5]; }
+
+// the warp's block row of the FP64 staging tile, as SpMV scratch
+template <class SM>
+__device__ __forceinline__ double* spmv_row(SM& sm) {
+  return sm.tile.d[0][threadIdx.x >> 5];
 }
 
 // max that propagates NaN (fmax drops it, which would let a blown-up
 // residual read as converged)
 __device__ __forceinline__ double nanmax(double a, double b) { return (a > b || a != a) ? a : b; }
 
-template <int NV>
-__device__ __forceinline__ void cta_partials(Smem& sm, const double (&v)[NV], unsigned is_max,
+template <int NV, class SM>
+__device__ __forceinline__ void cta_partials(SM& sm, const double (&v)[NV], unsigned is_max,
                                              double* __restrict__ red, int q0) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -130,8 +158,8 @@ __device__ __forceinline__ void cta_partials(Smem& sm, const double (&v)[NV], un
   }
 }
 
-template <int NV>
-__device__ __forceinline__ void grid_reduce(Smem& sm, unsigned is_max, const double* __restrict__ red, int q0) {
+template <int NV, class SM>
+__device__ __forceinline__ void grid_reduce(SM& sm, unsigned is_max, const double* __restrict__ red, int q0) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (w < NV) {
     const bool mx = (is_max >> w) & 1u;
@@ -158,28 +186,35 @@ template <class T>
 struct Pinv;
 
 // FP64: tiles of 8 blocks; warp w computes rows 8w..8w+7 with DMMA m8n8k4.
-// P^-1 stays in shared memory with padded rows: the A-fragment loads
-// (lane g,t reads row 8w+g, column 4kk+t) hit every bank pair once per
-// 16 lanes, the minimum two wavefronts for 32 doubles.
+// P^-1 stays in shared memory in rows of 64 doubles whose column c is stored
+// at c ^ 4*(r mod 8): the A-fragment loads (lane g,t reads row 8w+g, column
+// 4kk+t) hit every bank pair once per 16 lanes, the minimum two wavefronts
+// for 32 doubles.
 template <>
 struct Pinv<double> {
   static constexpr int kTile = 8;
-  const double (*P)[kPad];
+  const double (*P)[kBLEN];
+  __device__ __forceinline__ static int swz(int r, int c) { return c ^ ((r & 7) << 2); }
   // all threads; the caller synchronises before the first apply
-  __device__ __forceinline__ void load(PinvSmem& s, const double* __restrict__ Pg, const float*) {
-    for (int q = threadIdx.x; q < kBLEN * kBLEN; q += blockDim.x) s.d[q / kBLEN][q % kBLEN] = __ldg(Pg + q);
-    P = s.d;
+  __device__ __forceinline__ void load(PinvSmem<double>& s, const double* __restrict__ Pg, const float*) {
+    for (int q = threadIdx.x; q < kBLEN * kBLEN; q += blockDim.x) {
+      const int r = q / kBLEN, c = q % kBLEN;
+      s.v[r][swz(r, c)] = __ldg(Pg + q);
+    }
+    P = s.v;
   }
-  __device__ __forceinline__ static double (*rows(Smem& sm, int buf))[kPad] { return sm.tile.d[buf]; }
+  template <class SM>
+  __device__ __forceinline__ static double (*rows(SM& sm, int buf))[kPad] { return sm.tile.d[buf]; }
   __device__ __forceinline__ void apply(const double (*tile)[kPad], int w, int lane, int tb, int nvalid,
                                         double* __restrict__ z) const {
     const int g = lane >> 2, t = lane & 3;
-    const double* arow = P[8 * w + g];
+    const int r = 8 * w + g;  // r mod 8 == g
+    const double* arow = P[r];
     double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
 #pragma unroll
     for (int kk = 0; kk < 16; kk += 2) {
-      dmma_884(c0, c1, arow[4 * kk + t], tile[g][4 * kk + t]);
-      dmma_884(e0, e1, arow[4 * (kk + 1) + t], tile[g][4 * (kk + 1) + t]);
+      dmma_884(c0, c1, arow[swz(r, 4 * kk + t)], tile[g][4 * kk + t]);
+      dmma_884(e0, e1, arow[swz(r, 4 * (kk + 1) + t)], tile[g][4 * (kk + 1) + t]);
     }
     c0 += e0;
     c1 += e1;
@@ -205,38 +240,42 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 // FP32: tiles of 16 blocks; warp w computes rows 16*(w&3).. of blocks
 // 8*(w>>2).. with m16n8k8 TF32 MMA.  Operands are split x = hi + lo (both
 // TF32) and z = Phi*hi + Phi*lo + Plo*hi, accumulated in FP32, which keeps
-// the preconditioner apply at FP32 accuracy.
+// the preconditioner apply at FP32 accuracy.  The split P = Phi + Plo (TF32
+// bit patterns) is formed once, in rows of 64 words whose column c is
+// stored at c ^ 4*(r mod 8): the A-fragment loads (lane g, t reads row
+// 16m+g, column 8kk+t) then fall in 32 distinct banks.
 template <>
 struct Pinv<float> {
   static constexpr int kTile = 16;
-  const uint32_t (*Ph)[kPad];
-  const uint32_t (*Pl)[kPad];
-  // all threads; the caller synchronises before the first apply.  The split
-  // P = Phi + Plo (TF32 bit patterns) is formed once.
-  __device__ __forceinline__ void load(PinvSmem& s, const double*, const float* __restrict__ P32) {
+  const uint32_t (*Ph)[kBLEN];
+  const uint32_t (*Pl)[kBLEN];
+  __device__ __forceinline__ static int swz(int r, int c) { return c ^ ((r & 7) << 2); }
+  // all threads; the caller synchronises before the first apply
+  __device__ __forceinline__ void load(PinvSmem<float>& s, const double*, const float* __restrict__ P32) {
     for (int q = threadIdx.x; q < kBLEN * kBLEN; q += blockDim.x) {
+      const int r = q / kBLEN, c = q % kBLEN;
       const float v = __ldg(P32 + q);
       const uint32_t hi = to_tf32(v);
-      s.f[0][q / kBLEN][q % kBLEN] = hi;
-      s.f[1][q / kBLEN][q % kBLEN] = to_tf32(v - __uint_as_float(hi));
+      s.hi[r][swz(r, c)] = hi;
+      s.lo[r][swz(r, c)] = to_tf32(v - __uint_as_float(hi));
     }
-    Ph = s.f[0];
-    Pl = s.f[1];
+    Ph = s.hi;
+    Pl = s.lo;
   }
-  __device__ __forceinline__ static float (*rows(Smem& sm, int buf))[kPad] { return sm.tile.f[buf]; }
+  template <class SM>
+  __device__ __forceinline__ static float (*rows(SM& sm, int buf))[kPad] { return sm.tile.f[buf]; }
   __device__ __forceinline__ void apply(const float (*tile)[kPad], int w, int lane, int tb, int nvalid,
                                         float* __restrict__ z) const {
     const int g = lane >> 2, t = lane & 3, m = w & 3, nt = w >> 2;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     const float* brow = tile[8 * nt + g];
-    const int ra = 16 * m + g, rb = ra + 8;
+    const int ra = 16 * m + g, rb = ra + 8;  // ra mod 8 == rb mod 8: one swizzle for both
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
       const int c = 8 * kk + t;
-      // A fragment rows ra/rb, columns c/c+4: word address 4*row + col mod 32
-      // differs across the 32 lanes (row stride 68 words), conflict-free
-      const uint32_t ahi[4] = {Ph[ra][c], Ph[rb][c], Ph[ra][c + 4], Ph[rb][c + 4]};
-      const uint32_t alo[4] = {Pl[ra][c], Pl[rb][c], Pl[ra][c + 4], Pl[rb][c + 4]};
+      const int c0 = swz(ra, c), c1 = swz(ra, c + 4);
+      const uint32_t ahi[4] = {Ph[ra][c0], Ph[rb][c0], Ph[ra][c1], Ph[rb][c1]};
+      const uint32_t alo[4] = {Pl[ra][c0], Pl[rb][c0], Pl[ra][c1], Pl[rb][c1]};
       const float x0 = brow[c], x1 = brow[c + 4];
       const uint32_t h0 = to_tf32(x0), h1 = to_tf32(x1);
       const uint32_t l0 = to_tf32(x0 - __uint_as_float(h0)), l1 = to_tf32(x1 - __uint_as_float(h1));
@@ -282,26 +321,26 @@ struct EpiRhNu {
   T* nu;
   double acc;
   struct Pre {
-    T rh[LV];
+    T v[LV];  // rhat
   };
   __device__ __forceinline__ Pre load(int i0) const {
     Pre p;
-    ldv<LV>(rh + i0, p.rh);
+    ldv<LV>(rh + i0, p.v);
     return p;
   }
   __device__ __forceinline__ Pre load1(int i) const {
     Pre p{};
-    p.rh[0] = __ldcg(rh + i);
+    p.v[0] = __ldcg(rh + i);
     return p;
   }
   __device__ __forceinline__ void vec(int i0, const T (&y)[LV], const Pre& p) {
     stv<LV>(nu + i0, y);
 #pragma unroll
-    for (int j = 0; j < LV; ++j) acc += dprod(p.rh[j], y[j]);
+    for (int j = 0; j < LV; ++j) acc += dprod(p.v[j], y[j]);
   }
   __device__ __forceinline__ void one(int i, T y, const Pre& p, int j) {
     nu[i] = y;
-    acc += dprod(p.rh[j], y);
+    acc += dprod(p.v[j], y);
   }
 };
 
@@ -313,36 +352,37 @@ struct EpiTS {
   T* t;
   double ts, tt;
   struct Pre {
-    T s[LV];
+    T v[LV];  // s
   };
   __device__ __forceinline__ Pre load(int i0) const {
     Pre p;
-    ldv<LV>(s + i0, p.s);
+    ldv<LV>(s + i0, p.v);
     return p;
   }
   __device__ __forceinline__ Pre load1(int i) const {
     Pre p{};
-    p.s[0] = __ldcg(s + i);
+    p.v[0] = __ldcg(s + i);
     return p;
   }
   __device__ __forceinline__ void vec(int i0, const T (&y)[LV], const Pre& p) {
     stv<LV>(t + i0, y);
 #pragma unroll
     for (int j = 0; j < LV; ++j) {
-      ts += dprod(y[j], p.s[j]);
+      ts += dprod(y[j], p.v[j]);
       tt += dprod(y[j], y[j]);
     }
   }
   __device__ __forceinline__ void one(int i, T y, const Pre& p, int j) {
     t[i] = y;
-    ts += dprod(y, p.s[j]);
+    ts += dprod(y, p.v[j]);
     tt += dprod(y, y);
   }
 };
 
 // Mixed form: r = (b - mean_b) - A x in FP64, stored as FP32 (and as rhat
 // when set_rh); partials |r64|_inf, (rhat,r), |r|^2, |rhat|^2, |r32|_inf.
-__device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const double* __restrict__ b,
+template <class SM>
+__device__ __forceinline__ void true_residual(SM& sm, const MeshView& M, const double* __restrict__ b,
                                               double mean_b, const double* __restrict__ x, float* __restrict__ r,
                                               float* __restrict__ rh, bool set_rh, double* __restrict__ red,
                                               int b0, int b1, int r0, int r1) {
@@ -394,7 +434,7 @@ __device__ __forceinline__ void true_residual(Smem& sm, const MeshView& M, const
       if (set_rh) rh[i] = r32;
     }
   } epi{b, mean_b, r, rh, set_rh, {0.0, 0.0, 0.0, 0.0, 0.0}};
-  spmv_range<double>(M, x, b0, b1, r0, r1, epi, spmv_row<double>(sm));
+  spmv_range<double>(M, x, b0, b1, r0, r1, epi, spmv_row(sm));
   cta_partials<5>(sm, epi.v, 0x11u, red, Q_RU);
 }
 
@@ -411,7 +451,7 @@ struct MixedCtx {  // what the reliable update needs
 // X the solution type; RU enables the mixed form's true-residual
 // replacement.  Returns false if a barrier gave up.
 template <class T, bool RU>
-__device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, const Problem<T>& V,
+__device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, const Problem<T>& V,
                               double* __restrict__ red, int b0, int b1, int r0, int r1, const SolveParams& sp,
                               const MixedCtx& mx, IterState& st) {
   using X = double;
@@ -490,7 +530,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, cons
     // pass B: nu = A z; (rhat, nu)
     {
       EpiRhNu<T> epi{V.rh, V.nu, 0.0};
-      spmv_range<T>(M, V.z, b0, b1, r0, r1, epi, spmv_row<T>(sm));
+      spmv_range_staged<T>(M, V.z, V.rh, b0, b1, r0, r1, epi, spmv_stage(sm));
       const double v[1] = {epi.acc};
       cta_partials<1>(sm, v, 0u, red, Q_RHNU);
     }
@@ -536,7 +576,7 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, cons
     // pass D: t = A z2; (t,s), (t,t)
     {
       EpiTS<T> epi{V.r, V.t, 0.0, 0.0};
-      spmv_range<T>(M, V.z2, b0, b1, r0, r1, epi, spmv_row<T>(sm));
+      spmv_range_staged<T>(M, V.z2, V.r, b0, b1, r0, r1, epi, spmv_stage(sm));
       const double v[2] = {epi.ts, epi.tt};
       cta_partials<2>(sm, v, 0u, red, Q_TS);
     }
@@ -652,7 +692,8 @@ __device__ bool bicgstab_loop(Smem& sm, GridBarrier& B, const Pinv<T>& pin, cons
 
 // x -= sum(h^2 x)/sum(h^2) over the CTA's blocks (ExpAMRSolver.cpp:383-415);
 // x already holds the final iterate.
-__device__ bool subtract_mean(Smem& sm, GridBarrier& B, const MeshView& M, double* __restrict__ x,
+template <class SM>
+__device__ bool subtract_mean(SM& sm, GridBarrier& B, const MeshView& M, double* __restrict__ x,
                               double* __restrict__ red, int b0, int b1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double v[2] = {0.0, 0.0};
@@ -688,7 +729,8 @@ __device__ __forceinline__ void take_best(bool best_is_x, double* __restrict__ x
 
 // ============================================ one problem, one team ========
 
-__device__ __forceinline__ void write_stats(const Smem& sm, DevStats* stats, const IterState& st, int refinements,
+template <class SM>
+__device__ __forceinline__ void write_stats(const SM& sm, DevStats* stats, const IterState& st, int refinements,
                                             double err_final, double norm_ax0) {
   if (sm.team_rank == 0 && threadIdx.x == 0) {
     stats->status = st.status;
@@ -704,7 +746,7 @@ __device__ __forceinline__ void write_stats(const Smem& sm, DevStats* stats, con
 // Plain FP64 solve of one problem by the team: BiCGSTABSolver::main
 // (BiCGSTAB.cu:412-620) and the mean removal (ExpAMRSolver.cpp:383-415).
 // [b0,b1) is this CTA's block range, [r0,r1) its explicit rows.
-__device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
+__device__ bool solve_fp64(Smem<double>& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
                            const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
                            int r1) {
   const MeshView& M = pr.M;
@@ -748,7 +790,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
         rh[i] = rv;
       }
     } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
-    spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi, spmv_row<double>(sm));
+    spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi, spmv_row(sm));
     cta_partials<3>(sm, epi.v, 0x3u, red, Q_INIT);
   }
   if (!B.sync(&sm.flag, 0)) return false;
@@ -774,7 +816,7 @@ __device__ bool solve_fp64(Smem& sm, GridBarrier& B, const Pinv<double>& pin, co
 }
 
 // Mixed-precision solve of one problem by the team.
-__device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, const ProblemMixed& pr,
+__device__ bool solve_mixed(Smem<float>& sm, GridBarrier& B, const Pinv<float>& pin, const ProblemMixed& pr,
                             const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
                             int r1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -825,13 +867,22 @@ __device__ bool solve_mixed(Smem& sm, GridBarrier& B, const Pinv<float>& pin, co
 
 }  // namespace
 
+// The kernels' shared memory (P^-1, staging tiles and SpMV rings, reduction
+// scratch) is above the 48 KB of a static allocation: dynamic, sized
+// sizeof(Smem<T>) at every launch.
+extern __shared__ __align__(16) unsigned char g_solve_smem[];
+template <class T>
+__device__ __forceinline__ Smem<T>& solve_smem() {
+  return *reinterpret_cast<Smem<T>*>(g_solve_smem);
+}
+
 // ====================================================== single solves =====
 
 // Three CTAs per SM (80 registers): the passes are bound by per-warp memory
 // latency, and the extra warps outweigh the spills this costs (measured on
 // the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(const __grid_constant__ SolveArgs64 S) {
-  __shared__ Smem sm;
+  Smem<double>& sm = solve_smem<double>();
   const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
   const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
@@ -846,7 +897,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(c
 }
 
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(const __grid_constant__ SolveArgsMixed S) {
-  __shared__ Smem sm;
+  Smem<float>& sm = solve_smem<float>();
   const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
   const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
   GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
@@ -871,7 +922,8 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
 
 template <bool MIXED>
 __device__ __forceinline__ void batch_body(const BatchArgs& A) {
-  __shared__ Smem sm;
+  using KT = typename std::conditional<MIXED, float, double>::type;
+  Smem<KT>& sm = solve_smem<KT>();
   const int team = A.team;
   const int g = blockIdx.x / team, rank = blockIdx.x % team;
   GridBarrier B{A.bars + g, A.abort_flag, (unsigned)team, globaltimer_ns() + A.timeout_ns, 0u, A.prof,
@@ -928,11 +980,50 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_bat
 // ------------------------------------------------------------ launch -----
 
 namespace {
+const void* const kSolveFns[4] = {(const void*)k_bicgstab64, (const void*)k_bicgstab_mixed,
+                                  (const void*)k_bicgstab_batch64, (const void*)k_bicgstab_batch_mixed};
+
+size_t smem_bytes(const void* fn) {
+  return (fn == kSolveFns[1] || fn == kSolveFns[3]) ? sizeof(Smem<float>) : sizeof(Smem<double>);
+}
+
+// Allows the dynamic shared memory of a solve kernel on the current device
+// (once per device and kernel) and asks for the smallest shared-memory
+// carve-out that holds kSolveCtasPerSm of its CTAs, so that the rest of the
+// unified array stays L1.
+cudaError_t allow_smem(const void* fn) {
+  static unsigned done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int k = 0;
+  while (k < 4 && kSolveFns[k] != fn) ++k;
+  const unsigned bit = 1u << k;
+  if (dev >= 0 && dev < 64 && (__atomic_load_n(&done[dev], __ATOMIC_ACQUIRE) & bit)) return cudaSuccess;
+  const size_t bytes = smem_bytes(fn);
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  int per_sm = 0, reserved = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  if (e == cudaSuccess && per_sm > 0) {
+    const size_t need = (size_t)kSolveCtasPerSm * (bytes + (size_t)reserved);
+    const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / (size_t)per_sm);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  }
+  if (e == cudaSuccess && dev >= 0 && dev < 64) __atomic_fetch_or(&done[dev], bit, __ATOMIC_ACQ_REL);
+  return e;
+}
+
 int coop_grid(const void* fn, int device) {
-  int sms = 0, per_sm = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolveThreads, 0) != cudaSuccess) return 0;
-  return sms * per_sm;
+  int sms = 0, per_sm = 0, cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return 0;
+  if (cur != device && cudaSetDevice(device) != cudaSuccess) return 0;
+  const bool ok = allow_smem(fn) == cudaSuccess &&
+                  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+                  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSolveThreads, smem_bytes(fn)) ==
+                      cudaSuccess;
+  if (cur != device) cudaSetDevice(cur);
+  return ok ? sms * per_sm : 0;
 }
 }  // namespace
 
@@ -941,12 +1032,16 @@ int max_coop_grid_mixed(int device) { return coop_grid((const void*)k_bicgstab_m
 
 cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s) {
   void* args[] = {const_cast<SolveArgs64*>(&a)};
-  return cudaLaunchCooperativeKernel((const void*)k_bicgstab64, dim3(grid), dim3(kSolveThreads), args, 0, s);
+  if (cudaError_t e = allow_smem((const void*)k_bicgstab64)) return e;
+  return cudaLaunchCooperativeKernel((const void*)k_bicgstab64, dim3(grid), dim3(kSolveThreads), args,
+                                     sizeof(Smem<double>), s);
 }
 
 cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s) {
   void* args[] = {const_cast<SolveArgsMixed*>(&a)};
-  return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args, 0, s);
+  if (cudaError_t e = allow_smem((const void*)k_bicgstab_mixed)) return e;
+  return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args,
+                                     sizeof(Smem<float>), s);
 }
 
 int max_coop_grid_batch(int device, bool mixed) {
@@ -957,18 +1052,19 @@ int max_coop_grid_batch(int device, bool mixed) {
 // capture records the cooperative attribute in the graph's kernel node.
 cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s) {
   void* args[] = {const_cast<BatchArgs*>(&a)};
+  const void* fn = mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64;
+  if (cudaError_t e = allow_smem(fn)) return e;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kSolveThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem_bytes(fn);
   cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelExC(&cfg, mixed ? (const void*)k_bicgstab_batch_mixed : (const void*)k_bicgstab_batch64,
-                             args);
+  return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 // ------------------------------------------------------- single ops -------
@@ -976,7 +1072,7 @@ cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cuda
 __global__ void __launch_bounds__(kSolveThreads) k_precond64(const double* __restrict__ P, int nb,
                                                              const double* __restrict__ p, double* __restrict__ z) {
   __shared__ double tile[8][kPad];
-  __shared__ PinvSmem Ps;
+  __shared__ PinvSmem<double> Ps;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Pinv<double> pin;
   pin.load(Ps, P, nullptr);
@@ -1006,7 +1102,7 @@ cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, doubl
 __global__ void __launch_bounds__(kSolveThreads) k_precond32(const float* __restrict__ P32, int nb,
                                                              const float* __restrict__ p, float* __restrict__ z) {
   __shared__ float tile[16][kPad];
-  __shared__ PinvSmem Ps;
+  __shared__ PinvSmem<float> Ps;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Pinv<float> pin;
   pin.load(Ps, nullptr, P32);

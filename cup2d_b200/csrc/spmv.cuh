@@ -87,6 +87,19 @@ __device__ __forceinline__ void ldv(const T* p, T (&v)[N]) {
   }
 }
 
+// N consecutive values from shared memory as one 16-byte vector.
+template <int N, class T>
+__device__ __forceinline__ void lds16(const T* p, T (&v)[N]) {
+  static_assert(N * sizeof(T) == 16, "one 16-byte vector");
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    v[0] = a.x; v[1] = a.y;
+  }
+}
+
 template <int N, class T>
 __device__ __forceinline__ void stv(T* p, const T (&v)[N]) {
   static_assert(N * sizeof(T) % 8 == 0, "vector size");
@@ -259,6 +272,162 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
       cell = __ldg(M.rowcell + rn);
     }
   }
+}
+
+// ------------------------------------------- staged SpMV (passes B, D) ----
+//
+// The SpMV passes of the solve move 12-24 bytes per cell and were bound by
+// how many loads a warp keeps in flight: with the operands gathered into
+// registers a warp has one chunk outstanding.  Here every lane issues its
+// chunk's copies with cp.async (16-byte cells of the operand z and of the
+// epilogue's vector, the halo values across the block faces) into a
+// per-warp ring of kSpmvStages chunk slots in shared memory, kSpmvStages - 1 chunks
+// ahead of the one it computes; copies in flight hold no registers.  The
+// rows are then summed from shared memory in the same order as
+// stencil_chunk_smem (so both give the same bits).  The neighbour table of
+// the next chunk to issue is read into registers one step ahead (its halo
+// addresses depend on it).  The explicit rows are done between the first
+// copies and the first chunk, so that their dependent loads (offsets,
+// columns, gathered z) overlap the copies in flight.
+
+constexpr int kSpmvStages = 2;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// cp.async of B bytes (4, 8 or 16; both addresses B-aligned); n < B copies n
+// bytes and zero-fills the rest (n = 0: nothing is read).
+template <int B>
+__device__ __forceinline__ void cp_async_n(void* dst, const void* src, int n) {
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(B), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_n() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One warp's ring of chunk slots.
+template <class T>
+struct SpmvStage {
+  static constexpr int CB = Lane<T>::CB;
+  alignas(16) T z[kSpmvStages][CB * kBLEN];
+  alignas(16) T op[kSpmvStages][CB * kBLEN];
+  alignas(16) T halo[kSpmvStages][CB][4][kBS];  // 0 Xm (col 7 of the left block), 1 Xp (col 0), 2 Ym (row 7), 3 Yp (row 0)
+  alignas(16) int4 nb[kSpmvStages][CB];
+};
+
+// y = A z over blocks [b0, b1) and explicit rows [r0, r1) with the epilogue
+// operand `op` (the vector Epi's dot products read) staged beside z.  Epi
+// provides struct Pre { T v[V]; }, load1(i) for the explicit rows, vec() and
+// one() as for spmv_range.  `st` is this warp's stage ring.
+template <class T, class Epi>
+__device__ __forceinline__ void spmv_range_staged(const MeshView& M, const T* __restrict__ z,
+                                                  const T* __restrict__ op, int b0, int b1, int r0, int r1,
+                                                  Epi& epi, SpmvStage<T>& st) {
+  using Pre = typename Epi::Pre;
+  constexpr int V = Lane<T>::V, CB = Lane<T>::CB, S = kSpmvStages;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const Lane<T> L(lane);
+  // explicit rows: this thread's first row, its offsets and cell, early
+  int r = r0 + threadIdx.x;
+  int k0 = 0, k1 = 0;
+  int cell = 0;
+  if (r < r1) {
+    k0 = __ldg(M.xptr + r);
+    k1 = __ldg(M.xptr + r + 1);
+    cell = __ldg(M.rowcell + r);
+  }
+  const int nch = (b1 - b0 + CB - 1) / CB;
+  auto blk_of = [&](int k) { return b0 + (w + k * nw) * CB + L.bl; };
+  auto nbr_of = [&](int k) {
+    const int blk = blk_of(k);
+    return blk < b1 ? block_nbr(M, blk) : make_int4(kWall, kWall, kWall, kWall);
+  };
+  // the copies of the warp's k-th chunk into slot k % S
+  auto issue = [&](int k, const int4& nb) {
+    const int s = k % S, blk = blk_of(k);
+    const bool valid = blk < b1;
+    const int own = valid ? blk : b0;  // an address inside the range for zero-fills
+    cp_async_n<16>(&st.z[s][L.bl * kBLEN + L.cell0], z + own * kBLEN + L.cell0, valid ? 16 : 0);
+    cp_async_n<16>(&st.op[s][L.bl * kBLEN + L.cell0], op + own * kBLEN + L.cell0, valid ? 16 : 0);
+    if (L.sub == 0) st.nb[s][L.bl] = nb;
+    if (L.ix0 == 0 && nb.x >= 0)
+      cp_async_n<sizeof(T)>(&st.halo[s][L.bl][0][L.iy], z + nb.x * kBLEN + L.iy * kBS + (kBS - 1), sizeof(T));
+    if (L.ix0 + V == kBS && nb.y >= 0)
+      cp_async_n<sizeof(T)>(&st.halo[s][L.bl][1][L.iy], z + nb.y * kBLEN + L.iy * kBS, sizeof(T));
+    if (L.iy == 0 && nb.z >= 0)
+      cp_async_n<16>(&st.halo[s][L.bl][2][L.ix0], z + nb.z * kBLEN + (kBS - 1) * kBS + L.ix0, 16);
+    if (L.iy == kBS - 1 && nb.w >= 0)
+      cp_async_n<16>(&st.halo[s][L.bl][3][L.ix0], z + nb.w * kBLEN + L.ix0, 16);
+    cp_async_commit_group();
+  };
+  const int K = w < nch ? (nch - w + nw - 1) / nw : 0;  // chunks of this warp
+  // chunks 0 .. S-2 ahead (past the end: zero-fills only, an empty group)
+  if (K > 0) {
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k) issue(k, nbr_of(k));
+  }
+  int4 nn = nbr_of(S - 1);
+  // the explicit rows while the first chunks' copies are in flight: their
+  // dependent loads (offsets, columns, gathered z) overlap the copies
+  for (; r < r1; r += blockDim.x) {
+    const Pre pre = epi.load1(cell);
+    const T* __restrict__ vals = row_vals<T>(M);
+    T acc = T(0);
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
+    epi.one(cell, acc, pre, 0);
+    const int rn = r + blockDim.x;
+    if (rn < r1) {
+      k0 = __ldg(M.xptr + rn);
+      k1 = __ldg(M.xptr + rn + 1);
+      cell = __ldg(M.rowcell + rn);
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    cp_async_wait_n<S - 2>();  // this lane's copies of chunk k have landed
+    __syncwarp();              // ... and every lane's; slot (k+S-1)%S was last read in step k-1
+    issue(k + S - 1, nn);
+    nn = nbr_of(k + S);
+    const int s = k % S, blk = blk_of(k);
+    if (blk >= b1) continue;
+    const T* zs = &st.z[s][L.bl * kBLEN];
+    const T(*h)[kBS] = st.halo[s][L.bl];
+    const int4 nb = st.nb[s][L.bl];
+    T zc[V], dn[V], up[V];
+    Pre pre;
+    lds16<V>(zs + L.cell0, zc);
+    lds16<V>(&st.op[s][L.bl * kBLEN + L.cell0], pre.v);
+    const bool has_l = L.ix0 > 0 || nb.x >= 0, has_r = L.ix0 + V < kBS || nb.y >= 0;
+    const bool has_d = L.iy > 0 || nb.z >= 0, has_u = L.iy < kBS - 1 || nb.w >= 0;
+    const T vl = L.ix0 > 0 ? zs[L.cell0 - 1] : h[0][L.iy];
+    const T vr = L.ix0 + V < kBS ? zs[L.cell0 + V] : h[1][L.iy];
+    lds16<V>(L.iy > 0 ? zs + L.cell0 - kBS : &h[2][L.ix0], dn);
+    lds16<V>(L.iy < kBS - 1 ? zs + L.cell0 + kBS : &h[3][L.ix0], up);
+    T y[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      T a = T(0);
+      int n = 0;
+      if (j > 0) { a += zc[j - 1]; n++; } else if (has_l) { a += vl; n++; }
+      if (j < V - 1) { a += zc[j + 1]; n++; } else if (has_r) { a += vr; n++; }
+      if (has_d) { a += dn[j]; n++; }
+      if (has_u) { a += up[j]; n++; }
+      y[j] = a - T(n) * zc[j];
+    }
+    const int i0 = blk * kBLEN + L.cell0;
+    const unsigned mk = (unsigned)(explicit_mask<T>(M, blk, nb) >> L.cell0) & ((1u << V) - 1u);
+    if (mk == 0u) {
+      epi.vec(i0, y, pre);
+    } else {
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if (!((mk >> j) & 1u)) epi.one(i0 + j, y[j], pre, j);
+    }
+  }
+  cp_async_wait_n<0>();  // the empty tail groups; nothing may land after return
 }
 
 }  // namespace cup2d
