@@ -65,6 +65,12 @@ SIGNATURES = {
     "cup2d_pinv": (C.c_int, [P_f64]),
     "cup2d_poisson_create": (C.c_int, [C.POINTER(Forest), C.POINTER(SolveOpts), C.POINTER(C.c_void_p)]),
     "cup2d_poisson_update_mesh": (C.c_int, [C.c_void_p, C.POINTER(Forest)]),
+    "cup2d_poisson_adapt_disks": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_double,
+                                            C.POINTER(C.c_int64)]),
+    "cup2d_poisson_get_forest": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32)]),
+    "cup2d_poisson_pressure_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.POINTER(SolveStats), C.c_void_p]),
     "cup2d_poisson_set_opts": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts)]),
     "cup2d_poisson_num_cells": (C.c_int64, [C.c_void_p]),
     "cup2d_poisson_set_grid": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -78,6 +84,7 @@ SIGNATURES = {
     "cup2d_poisson_apply32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_precond32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cup2d_poisson_precond32_tc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup2d_poisson_export_csr": (C.c_int, [C.c_void_p, P_i64, P_i64, P_i64, P_i32, P_f64]),
     "cup2d_poisson_explicit_info": (C.c_int, [C.c_void_p, P_i64, P_i64]),
     "cup2d_poisson_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),

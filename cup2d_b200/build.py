@@ -17,7 +17,8 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libcup2d_poisson.so"
 
-SOURCES = ["assemble.cu", "bicgstab.cu", "capi.cu", "noalloc.cu", "server.cu", "timestep.cu", "spmv_staged.cu", "problems.cpp", "forest.cpp"]
+SOURCES = ["assemble.cu", "adapt.cu", "bicgstab.cu", "capi.cu", "noalloc.cu", "precond_tc.cu", "server.cu",
+           "timestep.cu", "spmv_staged.cu", "problems.cpp", "forest.cpp"]
 HEADERS = ["common.cuh", "kernels.hpp", "spmv.cuh", "handle_view.hpp", "forest.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -100,8 +100,16 @@ template <class T>
 struct DevBuf {
   T* p = nullptr;
   int64_t cap = 0;  // elements
-  int ensure(int64_t n) {
+  // Grows the buffer to n elements.  The old buffer is freed in stream order
+  // on `last_user` when given (the stream whose queued work may still read
+  // or write it), else on the allocation stream, where it must be idle.
+  int ensure(int64_t n, cudaStream_t last_user = nullptr) {
     if (n <= cap && p) return CUP2D_OK;
+    if (p && last_user) {
+      cudaFreeAsync(p, last_user);
+      p = nullptr;
+      cap = 0;
+    }
     release();
     const int64_t m = std::max<int64_t>(n, 1);
     cudaStream_t s = alloc_stream();
@@ -172,6 +180,11 @@ struct cup2d_poisson {
   DevBuf<DevStats> dstats;
   DevBuf<unsigned long long> prof;  // phase timers (profiling on)
   DevBuf<double> rhs_coef, rhs_part;  // device RHS: coefficients, partial sums + mean
+  // device forest adaptation: per-level states, Morton key marks and ranks,
+  // scan scratch, flag
+  DevBuf<uint8_t> ad_state;
+  DevBuf<int32_t> ad_mark, ad_rank, ad_scan, ad_flags;
+  DevBuf<double> ps_y, ps_part;  // pressure step: L(pold), weighted-mean partials
   uint64_t mesh_version = 0;
   bool profiling = false;
   int prof_grid = 0;                // grid of the profiled solves
@@ -228,13 +241,14 @@ int check_forest(const cup2d_forest* f) {
   return CUP2D_OK;
 }
 
-int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
-  int st = check_forest(f);
-  if (st) return st;
-  const int64_t nb = f->nblocks, n = nb * kBLEN;
+// Assembles the operator of the forest whose blocks are already in the
+// handle's level/bx/by buffers (nb of them), for the geometry of f (its
+// block arrays are not read).
+int assemble_blocks(cup2d_poisson* h, const cup2d_forest* f, int64_t nb) {
+  int st;
+  const int64_t n = nb * kBLEN;
   const int64_t entries = leaf_table_entries(f->bpdx, f->bpdy, f->level_max);
-  if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb)) ||
-      (st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
+  if ((st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
       (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
       (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
     return st;
@@ -242,10 +256,6 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   // by its first solve
   if ((st = h->xo.ensure(n))) return st;
   cudaStream_t s = h->stream;
-  if (cudaMemcpyAsync(h->level.p, f->level, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(h->bx.p, f->bx, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(h->by.p, f->by, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
   DeviceMesh& m = h->mesh;
   m.nb = nb;
   m.level = h->level.p;
@@ -277,6 +287,19 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   h->extent = f->extent;
   h->nb = nb;
   return CUP2D_OK;
+}
+
+int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
+  int st = check_forest(f);
+  if (st) return st;
+  const int64_t nb = f->nblocks;
+  if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb))) return st;
+  cudaStream_t s = h->stream;
+  if (cudaMemcpyAsync(h->level.p, f->level, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(h->bx.p, f->bx, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(h->by.p, f->by, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  return assemble_blocks(h, f, nb);
 }
 
 int ensure_scratch(cup2d_poisson* h) {
@@ -395,7 +418,9 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
     return CUP2D_CUDA_ERROR;
   }
   if (const char* e = std::getenv("CUP2D_GRID")) h->grid_override = std::atoi(e);
-  if ((st = shared_pinv(&h->P, &h->P32)) || (st = ensure_scratch(h))) {
+  // the no-allocation solve's static scratch is committed here, with the
+  // rest of the handle's memory, so that those solves never load or allocate
+  if ((st = shared_pinv(&h->P, &h->P32)) || (st = ensure_scratch(h)) || (st = noalloc_prepare(h->device))) {
     cup2d_poisson_destroy(h);
     return st;
   }
@@ -412,6 +437,66 @@ int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest) {
   // buffers may be reallocated: let solves queued on any stream finish first
   if (cudaDeviceSynchronize() != cudaSuccess) return CUP2D_CUDA_ERROR;
   return do_assemble(h, forest);
+}
+
+int cup2d_poisson_adapt_disks(cup2d_poisson* h, int32_t ndisks, const double* disks, double band,
+                              int64_t* nblocks) {
+  if (!h || h->nb <= 0 || ndisks < 0 || ndisks > kMaxAdaptDisks || (ndisks > 0 && !disks) || !(band >= 0.0))
+    return CUP2D_INVALID_ARGUMENT;
+  AdaptGeom g{};
+  g.bpdx = h->bpdx;
+  g.bpdy = h->bpdy;
+  g.L = h->level_max;
+  g.px = h->px;
+  g.py = h->py;
+  g.extent = h->extent;
+  int64_t off = 0;
+  for (int l = 0; l < h->level_max; ++l) {
+    g.off[l] = off;
+    off += ((int64_t)h->bpdx << l) * ((int64_t)h->bpdy << l);
+  }
+  g.off[h->level_max] = off;
+  AdaptDisks D{};
+  D.n = ndisks;
+  D.band = band;
+  for (int k = 0; k < ndisks; ++k)
+    for (int c = 0; c < 3; ++c) D.d[k][c] = disks[3 * k + c];
+  const int64_t K = adapt_key_space(h->bpdx, h->bpdy, h->level_max);
+  if (K > ((int64_t)1 << 30)) return CUP2D_BAD_MESH;  // key space beyond 4 GB
+  // buffers may be reallocated: let solves queued on any stream finish first
+  if (cudaDeviceSynchronize() != cudaSuccess) return CUP2D_CUDA_ERROR;
+  int st;
+  if ((st = h->ad_state.ensure(off)) || (st = h->ad_mark.ensure(K)) || (st = h->ad_rank.ensure(K + 1)) ||
+      (st = h->ad_scan.ensure(scan_temp_ints(K) + 2)) || (st = h->ad_flags.ensure(1)))
+    return st;
+  const AdaptScratch sc{h->ad_state.p, h->ad_mark.p, h->ad_rank.p, h->ad_scan.p, h->ad_flags.p};
+  int64_t nb = 0;
+  if ((st = adapt_build(g, D, sc, &nb, h->stream))) return st;
+  if (nb <= 0 || nb > (int64_t)(INT32_MAX / kBLEN)) return CUP2D_BAD_MESH;
+  if ((st = h->level.ensure(nb)) || (st = h->bx.ensure(nb)) || (st = h->by.ensure(nb))) return st;
+  if ((st = adapt_scatter(g, sc, nb, h->level.p, h->bx.p, h->by.p, h->stream))) return st;
+  cup2d_forest f{};
+  f.bpdx = h->bpdx;
+  f.bpdy = h->bpdy;
+  f.level_max = h->level_max;
+  f.periodic_x = h->px;
+  f.periodic_y = h->py;
+  f.extent = h->extent;
+  f.nblocks = nb;
+  if ((st = assemble_blocks(h, &f, nb))) return st;
+  if (nblocks) *nblocks = nb;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_get_forest(const cup2d_poisson* h, int32_t* level, int32_t* bx, int32_t* by) {
+  if (!h || h->nb <= 0 || !level || !bx || !by) return CUP2D_INVALID_ARGUMENT;
+  const size_t bytes = sizeof(int32_t) * (size_t)h->nb;
+  if (cudaMemcpyAsync(level, h->level.p, bytes, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaMemcpyAsync(bx, h->bx.p, bytes, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaMemcpyAsync(by, h->by.p, bytes, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
 }
 
 int cup2d_poisson_set_opts(cup2d_poisson* h, const cup2d_solve_opts* opts) {
@@ -492,7 +577,9 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
   unsigned long long* prof = nullptr;
   if (h->profiling) {
     const int64_t words = (int64_t)grid * kProfPhases * 2;
-    if ((st = h->prof.ensure(words))) return st;
+    // sized once for the handle's largest grid, so it never grows under
+    // solves still queued on a stream
+    if ((st = h->prof.ensure((int64_t)std::max(h->grid64, h->gridmx) * kProfPhases * 2))) return st;
     if (h->prof_grid != grid) {  // timers accumulate over solves of one grid size
       if (cudaMemsetAsync(h->prof.p, 0, sizeof(unsigned long long) * words, s) != cudaSuccess)
         return CUP2D_CUDA_ERROR;
@@ -574,6 +661,27 @@ int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* 
   return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, h->err.p, s));
 }
 
+int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres, double* d_pold,
+                                cup2d_solve_stats* stats, void* stream) {
+  if (!h || !d_tmp || !d_pres || !d_pold || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_tmp) || !aligned16(d_pres) || !aligned16(d_pold)) return CUP2D_INVALID_ARGUMENT;
+  if (d_tmp == d_pres || d_tmp == d_pold || d_pres == d_pold) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+  const int64_t n = h->nb * kBLEN;
+  int st;
+  if ((st = h->ps_y.ensure(n, s)) || (st = h->ps_part.ensure(wmean_partials(h->nb), s))) return st;
+  // POLD = PRES (PressureSingle.cpp:836-846); tmp -= L(pold), PRES = 0 (:847-848, 411-418)
+  if (cudaMemcpyAsync(d_pold, d_pres, sizeof(double) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  if (launch_spmv64(h->mesh.view(), d_pold, h->ps_y.p, h->err.p, s) != cudaSuccess ||
+      launch_rhs_minus_lpold(d_tmp, h->ps_y.p, d_pres, n, s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  // pressureSolver->solve(sim.tmp, sim.pres) (:850)
+  if ((st = cup2d_poisson_solve_device(h, d_tmp, d_pres, stats, stream))) return st;
+  // PRES += POLD - mean(PRES), volume-weighted (:853-879)
+  return from_cuda(launch_add_pold(d_pres, d_pold, h->hblk.p, h->nb, h->ps_part.p, s));
+}
+
 int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream) {
   if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
@@ -614,7 +722,11 @@ int cup2d_poisson_rhs_fourier_device(cup2d_poisson* h, int32_t kmax, const doubl
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nm = fourier_mode_count(kmax);
   int st;
-  if ((st = h->rhs_coef.ensure(4 * nm)) || (st = h->rhs_part.ensure(rhs_partials(h->nb) + 1))) return st;
+  // coefficients: sized for the largest kmax once; partials: grow with the
+  // mesh, the old buffer freed behind the work already queued on s
+  if ((st = h->rhs_coef.ensure(4 * (int64_t)fourier_mode_count(kMaxFourierK))) ||
+      (st = h->rhs_part.ensure(rhs_partials(h->nb) + 1, s)))
+    return st;
   if (cudaMemcpyAsync(h->rhs_coef.p, coef, sizeof(double) * 4 * nm, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
   const int64_t parts = rhs_partials(h->nb);
@@ -643,6 +755,18 @@ int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void
   if (!h || !d_p || !d_z) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
   return from_cuda(launch_precond32(h->P32, h->nb, d_p, d_z, s));
+}
+
+int cup2d_poisson_precond32_tc(cup2d_poisson* h, const float* d_p, float* d_z, void* stream) {
+  if (!h || !d_p || !d_z || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+  if (cudaMemsetAsync(h->err.p, 0, sizeof(int), s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  if (launch_precond32_tc(h->P32, h->nb, d_p, d_z, h->err.p, s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  int err = 0;
+  if (cudaMemcpyAsync(&err, h->err.p, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return CUP2D_CUDA_ERROR;
+  return err ? CUP2D_TIMEOUT : CUP2D_OK;
 }
 
 int cup2d_poisson_set_profiling(cup2d_poisson* h, int32_t enable) {
@@ -1045,7 +1169,8 @@ int cup2d_batch_solve_device(cup2d_batch* B, const double* const* d_b, double* c
     return CUP2D_CUDA_ERROR;
   if (B->profiling) {
     const int64_t words = (int64_t)grid * kProfPhases * 2;
-    if ((st = B->prof.ensure(words))) return st;
+    // sized once for the batch's largest grid (see the single-solve timers)
+    if ((st = B->prof.ensure((int64_t)std::max(B->grid64, B->gridmx) * kProfPhases * 2))) return st;
     if (B->prof_grid != grid) {  // timers accumulate over launches of one grid size
       if (cudaMemsetAsync(B->prof.p, 0, sizeof(unsigned long long) * words, s) != cudaSuccess)
         return CUP2D_CUDA_ERROR;

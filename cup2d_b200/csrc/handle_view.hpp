@@ -38,5 +38,9 @@ size_t handle_stats_bytes();
 int handle_destroy_idle(cup2d_poisson* h);
 // Statistics from a `raw` record filled by handle_solve_async.
 void handle_stats_from_raw(const void* raw, double solve_ms, cup2d_solve_stats* out);
+// Looks up (once per device, with that device current) the address of the
+// static scratch array of cup2d_poisson_solve_device_noalloc, which commits
+// the array on that device (noalloc.cu).
+int noalloc_prepare(int device);
 
 }  // namespace cup2d

@@ -177,6 +177,8 @@ cudaError_t launch_spmv64(const MeshView& M, const double* x, double* y, int* er
 cudaError_t launch_spmv32(const MeshView& M, const float* x, float* y, int* err, cudaStream_t s);
 cudaError_t launch_precond64(const double* P, int64_t nb, const double* p, double* z, cudaStream_t s);
 cudaError_t launch_precond32(const float* P32, int64_t nb, const float* p, float* z, cudaStream_t s);
+// The same apply on tcgen05 tensor cores with TMEM accumulators (precond_tc.cu).
+cudaError_t launch_precond32_tc(const float* P32, int64_t nb, const float* p, float* z, int* err, cudaStream_t s);
 
 // Forest of a handle on the device: per-block level and coordinates, and the
 // per-level dense leaf tables (block id or -1, level l at off[l], row-major
@@ -192,6 +194,38 @@ struct ForestView {
   int64_t off[kMaxLevels + 1];
 };
 
+// Forest adaptation on the device (adapt.cu).  States are dense per-level
+// byte arrays at the offsets of the leaf tables.
+constexpr int kMaxAdaptDisks = 64;
+struct AdaptGeom {
+  int32_t bpdx, bpdy, L, px, py;
+  double extent;
+  int64_t off[kMaxLevels + 1];
+};
+struct AdaptDisks {
+  int32_t n;
+  double band;
+  double d[kMaxAdaptDisks][3];  // cx, cy, r
+};
+struct AdaptScratch {
+  uint8_t* state;    // [leaf_table_entries]
+  int32_t* mark;     // [adapt_key_space]
+  int32_t* rank;     // [adapt_key_space + 1]: exclusive prefix sums, then the total
+  int32_t* scan_tmp; // [scan_temp_ints(adapt_key_space)]
+  int* changed;      // [1]: balance round flag, scatter error flag
+};
+// Size of the dense Morton key space of a forest's leaves (a power of 4).
+int64_t adapt_key_space(int bpdx, int bpdy, int level_max);
+// Tags, balances and orders the leaves; returns their number in *nleaves
+// (read back: the caller sizes the block arrays with it).  CUP2D_OK,
+// CUP2D_CUDA_ERROR, or CUP2D_BAD_MESH if the balance did not settle.
+int adapt_build(const AdaptGeom& g, const AdaptDisks& D, const AdaptScratch& sc, int64_t* nleaves,
+                cudaStream_t s);
+// Writes the nb leaves (level, bx, by) in Morton order (CUP2D_OK, or an error
+// status; synchronises the stream).
+int adapt_scatter(const AdaptGeom& g, const AdaptScratch& sc, int64_t nb, int32_t* level, int32_t* bx, int32_t* by,
+                  cudaStream_t s);
+
 // Time-stepping steps around the solve (timestep.cu).
 constexpr int kMaxFourierK = 24;
 int fourier_mode_count(int kmax);
@@ -200,6 +234,13 @@ int64_t rhs_partials(int64_t nb);  // scratch doubles of launch_rhs_fourier
 // (device, 4 per mode); partial [rhs_partials(nb)] and mean [1] scratch.
 cudaError_t launch_rhs_fourier(const ForestView& F, int kmax, const double* coef, double* b, double* partial,
                                double* mean, cudaStream_t s);
+// Pressure step around the solve (PressureSingle.cpp:831-879): tmp -= y and
+// pres = 0; then pres += pold - (volume-weighted mean of pres), with
+// `partial` scratch of wmean_partials(nb) doubles.
+cudaError_t launch_rhs_minus_lpold(double* tmp, const double* y, double* pres, int64_t n, cudaStream_t s);
+int64_t wmean_partials(int64_t nb);
+cudaError_t launch_add_pold(double* pres, const double* pold, const double* hblk, int64_t nb, double* partial,
+                            cudaStream_t s);
 // xd (on D) = xs (on S) carried across a change of forest.
 cudaError_t launch_transfer(const ForestView& S, const double* xs, const ForestView& D, double* xd,
                             cudaStream_t s);

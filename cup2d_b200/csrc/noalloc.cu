@@ -15,14 +15,20 @@
 // Limits and rules (also in include/cup2d_poisson.h):
 //  * at most kNoAllocMaxBlocks = 4096 blocks (262,144 cells) and 1024 CTAs;
 //    larger problems are rejected with CUP2D_INVALID_ARGUMENT;
-//  * the array is 16.2 MiB of static device memory that every GPU which
-//    loads the library holds until the process exits;
+//  * the array is 16.2 MiB of static device memory, committed on a GPU when
+//    the first handle is created there and held until the process exits;
 //  * all calls share the array, which keeps the last call's contents; calls
 //    whose work overlaps on the GPU (other streams, other threads) race, so
 //    callers serialise them;
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make
-//    that first call before any stream capture.
+//  * the array's device address is looked up with cudaGetSymbolAddress, once
+//    per device, when the first handle is created on that device
+//    (cup2d_poisson_create calls noalloc_prepare with the device current).
+//    Under CUDA's lazy module loading (the default) that lookup is what
+//    loads this file's module and commits the array, so the memory is taken
+//    at handle creation, where allocating is expected, and never inside a
+//    no-allocation solve.  A solve on a device without a prepared address
+//    (not expected) looks it up itself; that path may allocate, so it is
+//    not meant to run inside a stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -65,8 +71,10 @@ namespace {
 std::mutex g_scratch_mu;
 char* g_scratch_base[kMaxDevices] = {};
 
+}  // namespace
+
 // Device address of the scratch on the current device (looked up once).
-int scratch_base(int device, char** out) {
+int noalloc_scratch_base(int device, char** out) {
   if (device < 0 || device >= kMaxDevices) return CUP2D_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   if (!g_scratch_base[device]) {
@@ -82,7 +90,11 @@ int scratch_base(int device, char** out) {
   return CUP2D_OK;
 }
 
-}  // namespace
+int noalloc_prepare(int device) {
+  char* base = nullptr;
+  return noalloc_scratch_base(device, &base);
+}
+
 }  // namespace cup2d
 
 extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, double* d_x,
@@ -96,7 +108,7 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   int current = -1;
   if (cudaGetDevice(&current) != cudaSuccess || current != v.device) return CUP2D_INVALID_ARGUMENT;
   char* base = nullptr;
-  int st = scratch_base(current, &base);
+  int st = noalloc_scratch_base(current, &base);
   if (st != CUP2D_OK) return st;
   const cup2d_solve_opts& o = v.opts;
   const int grid = std::max(1, std::min(v.grid, kNoAllocMaxGrid));

@@ -158,7 +158,104 @@ __global__ void k_transfer(ForestView S, const double* __restrict__ xs, ForestVi
   xd[cell] = 0.25 * acc;
 }
 
+// ------------------------------------------------ pressure step helpers --
+
+// tmp -= y (y = L(pold), the assembled operator applied to the old pressure:
+// updatePressureRHS1, PressureSingle.cpp:411-418), and pres = 0.
+__global__ void k_rhs_minus_lpold(double* __restrict__ tmp, const double* __restrict__ y,
+                                  double* __restrict__ pres, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    tmp[i] -= y[i];
+    pres[i] = 0.0;
+  }
+}
+
+// Per-CTA partial sums of h^2 p and of h^2 over the cells (the volume
+// weights of PressureSingle.cpp:853-868), in a fixed order.
+__global__ void __launch_bounds__(kRhsThreads) k_wsum_partials(const double* __restrict__ p,
+                                                               const double* __restrict__ hblk, int64_t n,
+                                                               double* __restrict__ partial) {
+  const int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v = 0.0, w = 0.0;
+  if (cell < n) {
+    const double h = hblk[cell >> 6];
+    w = h * h;
+    v = p[cell] * w;
+  }
+  __shared__ double ws[2][kRhsThreads / 32];
+  v = warp_sum(v);
+  w = warp_sum(w);
+  if ((threadIdx.x & 31) == 0) {
+    ws[0][threadIdx.x >> 5] = v;
+    ws[1][threadIdx.x >> 5] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < kRhsThreads / 32; ++k) {
+      a += ws[0][k];
+      b += ws[1][k];
+    }
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// One CTA: avg = sum(h^2 p) / sum(h^2) from the partials (fixed order).
+__global__ void __launch_bounds__(256) k_wmean(const double* __restrict__ partial, int64_t nparts,
+                                               double* __restrict__ avg) {
+  __shared__ double ws[2][8];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = threadIdx.x; i < nparts; i += blockDim.x) {
+    a += partial[2 * i];
+    b += partial[2 * i + 1];
+  }
+  a = warp_sum(a);
+  b = warp_sum(b);
+  if ((threadIdx.x & 31) == 0) {
+    ws[0][threadIdx.x >> 5] = a;
+    ws[1][threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int k = 0; k < 8; ++k) {
+      sa += ws[0][k];
+      sb += ws[1][k];
+    }
+    *avg = sa / sb;
+  }
+}
+
+// pres += pold - avg (PressureSingle.cpp:869-879)
+__global__ void k_add_pold(double* __restrict__ pres, const double* __restrict__ pold, int64_t n,
+                           const double* __restrict__ avg) {
+  const double a = *avg;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    pres[i] += pold[i] - a;
+}
+
 }  // namespace
+
+cudaError_t launch_rhs_minus_lpold(double* tmp, const double* y, double* pres, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_rhs_minus_lpold<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(tmp, y, pres, n);
+  return cudaGetLastError();
+}
+
+int64_t wmean_partials(int64_t nb) { return 2 * ((nb * kBLEN + kRhsThreads - 1) / kRhsThreads) + 1; }
+
+cudaError_t launch_add_pold(double* pres, const double* pold, const double* hblk, int64_t nb, double* partial,
+                            cudaStream_t s) {
+  const int64_t n = nb * kBLEN;
+  if (n <= 0) return cudaSuccess;
+  const int64_t parts = (n + kRhsThreads - 1) / kRhsThreads;
+  double* avg = partial + 2 * parts;
+  k_wsum_partials<<<(unsigned)parts, kRhsThreads, 0, s>>>(pres, hblk, n, partial);
+  k_wmean<<<1, 256, 0, s>>>(partial, parts, avg);
+  k_add_pold<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(pres, pold, n, avg);
+  return cudaGetLastError();
+}
 
 int fourier_mode_count(int kmax) {
   int n = 0;

@@ -88,6 +88,28 @@ class Solver:
         f = mesh.forest()
         L.check(L.lib().cup2d_poisson_update_mesh(self._h, C.byref(f)), "cup2d_poisson_update_mesh")
 
+    def adapt_disks(self, disks, band: float) -> Mesh:
+        """Re-adapts the forest on the device to the disk geometry (refined
+        to the finest level within `band` of each disk, 2:1 balanced, Morton
+        order: the forest Mesh.disks builds on the host for this handle's
+        root grid, levels, extent and periodicity) and re-assembles the
+        operator.  Returns the new forest (read back from the device)."""
+        d = np.ascontiguousarray(np.asarray(disks, dtype=np.float64).reshape(-1, 3))
+        nb = C.c_int64()
+        L.check(L.lib().cup2d_poisson_adapt_disks(self._h, d.shape[0], _pd(d), float(band), C.byref(nb)),
+                "cup2d_poisson_adapt_disks")
+        self.mesh = self.device_forest()
+        return self.mesh
+
+    def device_forest(self) -> Mesh:
+        """The handle's current forest, read back from the device."""
+        nb = self.ncells // 64
+        lv, bx, by = (np.empty(nb, dtype=np.int32) for _ in range(3))
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))  # noqa: E731
+        L.check(L.lib().cup2d_poisson_get_forest(self._h, p(lv), p(bx), p(by)), "cup2d_poisson_get_forest")
+        m = self.mesh
+        return Mesh(m.bpdx, m.bpdy, m.level_max, m.extent, lv, bx, by, m.periodic_x, m.periodic_y)
+
     def set_opts(self, opts: Optional[L.SolveOpts] = None, **kw) -> None:
         self.opts = opts if opts is not None else make_opts(**kw)
         L.check(L.lib().cup2d_poisson_set_opts(self._h, C.byref(self.opts)), "cup2d_poisson_set_opts")
@@ -128,6 +150,20 @@ class Solver:
             self.last_stats = st.as_dict()
             return self.last_stats
         return None
+
+    def pressure_step(self, tmp, pres, pold, stream=None) -> dict:
+        """PressureSingle's step around the solve on device tensors:
+        pold = pres; tmp -= L(pold); pres = solve(tmp); pres += pold - mean.
+        Returns the solve's statistics (the call synchronises)."""
+        for t in (tmp, pres, pold):
+            _check_dev(t, self.ncells)
+        st = L.SolveStats()
+        L.check(L.lib().cup2d_poisson_pressure_step(self._h, C.c_void_p(tmp.data_ptr()), C.c_void_p(pres.data_ptr()),
+                                                     C.c_void_p(pold.data_ptr()), C.byref(st),
+                                                     _stream_handle(stream)),
+                "cup2d_poisson_pressure_step")
+        self.last_stats = st.as_dict()
+        return self.last_stats
 
     def solve_device_noalloc(self, b, x, stream=None) -> dict:
         """The FP64 device solve without any device allocation, for callers
@@ -173,8 +209,14 @@ class Solver:
                                                C.c_void_p(x_dst.data_ptr()), _stream_handle(stream)),
                 "cup2d_poisson_transfer")
 
-    def precond(self, p, z, stream=None) -> None:
-        fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond
+    def precond(self, p, z, stream=None, tcgen05: bool = False) -> None:
+        """z = P^-1 p per block: FP64, or FP32 (split TF32) on float32 tensors;
+        tcgen05=True takes the FP32 apply on the tcgen05 tensor cores (TMEM
+        accumulators) instead of mma.sync."""
+        if tcgen05:
+            fn = L.lib().cup2d_poisson_precond32_tc
+        else:
+            fn = L.lib().cup2d_poisson_precond32 if str(p.dtype) == "torch.float32" else L.lib().cup2d_poisson_precond
         s = _stream_handle(stream)
         L.check(fn(self._h, C.c_void_p(p.data_ptr()), C.c_void_p(z.data_ptr()), s), "cup2d_poisson_precond")
 

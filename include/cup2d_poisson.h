@@ -114,6 +114,25 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
                          cup2d_poisson** out);
 /* Re-assembly after mesh adaptation (the UpdateFluxCorrection branch). */
 int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest);
+/* Mesh adaptation on the device, then re-assembly: the role of
+ * AdaptTheMesh::adapt (source/Operators/AdaptTheMesh.cpp:80-110: tag, then
+ * Cubism's refinement/compression and 2:1 balance) followed by the
+ * UpdateFluxCorrection branch of ExpAMRSolver::solve
+ * (source/Poisson/ExpAMRSolver.cpp:370-376), for the benchmark's geometric
+ * criterion.  The handle's forest is replaced by the one cup2d_mesh_disks
+ * builds for the handle's bpdx, bpdy, level_max, extent and periodicity:
+ * blocks meeting the band | |p - c| - r | <= band of a disk refined to
+ * level_max - 1, 2:1 balanced across faces and corners, Morton-ordered --
+ * built on the device (no host forest, one read-back of the block count)
+ * and assembled as update_mesh does.  disks: host array of ndisks
+ * (cx, cy, r) triples, ndisks <= 64.  *nblocks receives the new block count
+ * (NULL to ignore).  Like update_mesh, it waits for the device first. */
+int cup2d_poisson_adapt_disks(cup2d_poisson* h, int32_t ndisks, const double* disks, double band,
+                              int64_t* nblocks);
+/* The handle's current forest, in the block order of its vectors: level and
+ * (i, j) index of each of its cup2d_poisson_num_cells/64 blocks (host
+ * arrays). */
+int cup2d_poisson_get_forest(const cup2d_poisson* h, int32_t* level, int32_t* bx, int32_t* by);
 int cup2d_poisson_set_opts(cup2d_poisson* h, const cup2d_solve_opts* opts);
 int64_t cup2d_poisson_num_cells(const cup2d_poisson* h);
 /* Number of CTAs of the persistent solve kernels (0 = size heuristic).  The
@@ -137,13 +156,15 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
  * device-wide synchronisation cudaMalloc/cudaFree can cause.  The handle's
  * operator (built at create/update time) and the caller's b and x are the
  * inputs and outputs; every scratch buffer of the solve lives in one static
- * device array of 16.2 MiB that each GPU loading the library holds until
- * exit.  Limits: at most CUP2D_NOALLOC_MAX_BLOCKS blocks (larger problems
- * return CUP2D_INVALID_ARGUMENT) and always the plain FP64 form.  All calls
- * share the array: calls whose GPU work overlaps race, so serialise them.
- * The first call on a device looks up the array's address (the handle's
- * device must be current); make it before any stream capture.  Otherwise
- * behaves as cup2d_poisson_solve_device. */
+ * device array of 16.2 MiB.  The array is committed on a GPU when the first
+ * handle is created there (cup2d_poisson_create looks up its address, which
+ * under CUDA's lazy module loading loads and allocates it) and held until
+ * exit, so the solve itself loads and allocates nothing.  Limits: at most
+ * CUP2D_NOALLOC_MAX_BLOCKS blocks (larger problems return
+ * CUP2D_INVALID_ARGUMENT) and always the plain FP64 form.  All calls share
+ * the array, which keeps the last call's contents: calls whose GPU work
+ * overlaps race, so serialise them.  The handle's device must be current.
+ * Otherwise behaves as cup2d_poisson_solve_device. */
 #define CUP2D_NOALLOC_MAX_BLOCKS 4096
 int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double* d_b, double* d_x,
                                        cup2d_solve_stats* stats, void* stream);
@@ -169,9 +190,30 @@ int cup2d_poisson_rhs_fourier_device(cup2d_poisson* h, int32_t kmax, const doubl
                                      void* stream);
 int cup2d_poisson_transfer(const cup2d_poisson* src, const double* d_xsrc, const cup2d_poisson* dst,
                            double* d_xdst, void* stream);
+/* The pressure step around the solve, as PressureSingle::operator() runs it
+ * (source/Operators/PressureSingle.cpp:831-879), on device buffers:
+ *   pold = pres; tmp -= L(pold); pres = 0            (:836-848, 411-418)
+ *   solve L pres = tmp (cup2d_poisson_solve_device)  (:850)
+ *   pres += pold - mean(pres), volume-weighted       (:853-879)
+ * L is the assembled operator (the same rows updatePressureRHS1 applies with
+ * Cubism's ghost cells and flux correction).  On entry d_tmp holds the
+ * divergence part of the right-hand side (updatePressureRHS) and d_pres the
+ * previous pressure; on return d_pres holds the new pressure, d_pold the
+ * previous one and d_tmp the right-hand side that was solved.  The three
+ * buffers must be distinct.  Asynchronous on `stream` unless stats != NULL,
+ * when the solve's statistics are read back (the final update stays
+ * queued on the stream). */
+int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres, double* d_pold,
+                                cup2d_solve_stats* stats, void* stream);
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
 /* FP32 P^-1 apply of the mixed form (split-TF32 tensor-core MMA). */
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);
+/* The same FP32 P^-1 apply on the 5th-generation tensor cores (tcgen05.mma,
+ * accumulators in tensor memory): the cublasDgemm of P_inv
+ * (source/Poisson/BiCGSTAB.cu:520,545) in the mixed form's precision,
+ * measured beside cup2d_poisson_precond32.  Synchronises the stream;
+ * CUP2D_TIMEOUT if the tensor-core work did not complete within 2 s. */
+int cup2d_poisson_precond32_tc(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);
 /* The assembled operator as CSR (host buffers).  Call with NULL arrays to
  * get n and nnz. */
 int cup2d_poisson_export_csr(cup2d_poisson* h, int64_t* n, int64_t* nnz,

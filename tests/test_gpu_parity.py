@@ -262,3 +262,28 @@ def test_timeout_status(cuda):
         s.set_opts(tol_rel=1e-6, max_iter=5000)
         s.solve(b)
         assert s.last_stats["status"] == L.OK
+
+
+@pytest.mark.parametrize("name", ["sized_400", "single_block", "sized_1500"])
+def test_precond32_tcgen05_matches(cuda, name):
+    """The FP32 P^-1 apply on tcgen05 tensor cores (TMEM accumulators) against
+    the oracle's FP64 apply (FP32 accuracy) and the mma.sync apply; block
+    counts that are not multiples of its 32-block tile exercise the partial
+    last tile."""
+    import torch
+    m = MESHES[name]
+    rng = np.random.default_rng(3)
+    p = rng.standard_normal(m.ncells).astype(np.float32)
+    z_o = oracle.precond(oracle.pinv(), p.astype(np.float64))
+    with Solver(m) as s:
+        p32 = torch.from_numpy(p).to(cuda)
+        z_tc = torch.full_like(p32, float("nan"))
+        z_ms = torch.empty_like(p32)
+        s.precond(p32, z_tc, tcgen05=True)
+        s.precond(p32, z_ms)
+        torch.cuda.synchronize()
+        a = z_tc.double().cpu().numpy()
+        b = z_ms.double().cpu().numpy()
+    assert np.all(np.isfinite(a))
+    assert np.max(np.abs(a - z_o)) <= 2e-6 * np.max(np.abs(z_o))
+    assert np.max(np.abs(a - b)) <= 2e-6 * np.max(np.abs(z_o))

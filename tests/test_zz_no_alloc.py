@@ -4,8 +4,9 @@ cup2d_poisson_solve_device_noalloc serves callers that must not allocate
 device memory at solve time (device memory owned by their own pool, or a loop
 that cannot afford an allocation's synchronisation).  Its scratch is one
 static device array shared by every call, so this file checks two calls in
-a row (the second sees the first one's leftovers), the size limit, and that
-the results match the allocating entry point.  It is collected last so that a
+a row (the second sees the first one's leftovers), that the device's free
+memory does not change across a call, the size limit, and that the results
+match the allocating entry point.  It is collected last so that a
 run stopping at the first failure has already run every other test.
 """
 import ctypes as C
@@ -38,11 +39,17 @@ def test_noalloc_matches_allocating_solve(cuda, mesh_fn):
             assert st["status"] == L.OK
             ref.append((x.cpu().numpy(), st))
         # two calls in a row through the C ABI; the second reuses the static
-        # scratch the first one left behind
+        # scratch the first one left behind.  The device's free memory is
+        # the same before and after each call: the static array was
+        # committed when the handle was created, and the call allocates
+        # nothing (no pool growth, no module load).
         for (x_ref, st_ref), b in zip(ref, rhs):
             x = torch.zeros_like(b)
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             st = s.solve_device_noalloc(b, x)
             torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free_before
             assert st["status"] == L.OK, st
             assert st["rel_res_inf"] <= 1e-8
             # same kernel, grid and block ranges: the result matches the
