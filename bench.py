@@ -705,7 +705,8 @@ def run_serve_sweep(args) -> dict:
     return {"metric": "served Poisson solves/s (open-loop arrivals), offered-rate sweep", "unit": UNIT,
             "sweep": [{"offered_rate": d["offered_rate"], "served": d["value"], "latency_ms": d["latency_ms"],
                        "status_ok": d["status_ok"], "device_busy": d["device_busy"],
-                       "assemblies": d["server"]["assemblies"]} for d in legs],
+                       "assemblies": d["server"]["assemblies"], "assembly_ms_mean": d["assembly_ms_mean"]}
+                      for d in legs],
             "saturation": {"served": best["value"], "at_offered_rate": best["offered_rate"]},
             "config": legs[0]["config"], "requests_per_rate": args.serve_requests}
 
@@ -795,7 +796,8 @@ def run_serve(args) -> dict:
                       f"mesh with a new RHS, 70% a new mesh id (assembled on admission); mixed, rel. 1e-6, "
                       f"x0 = 0; {args.serve_inflight} solve slots, team = blocks/{args.serve_bpc} (2..128)",
             "server": {k2: c[k2] for k2 in ("admitted", "completed", "failed", "assemblies", "evictions",
-                                            "resident_meshes")}}
+                                            "resident_meshes")},
+            "assembly_ms_mean": c["assembly_us"] / 1e3 / max(1, c["assemblies"])}
 
 
 def cpu_baseline(mesh, seeds) -> dict:

@@ -37,7 +37,7 @@ class SolveOpts(C.Structure):
 class ServerCounters(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "failed", "queued", "inflight",
                                         "resident_meshes", "evictions", "assemblies", "resident_bytes",
-                                        "budget_bytes")]
+                                        "budget_bytes", "assembly_us")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

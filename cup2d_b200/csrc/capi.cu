@@ -406,7 +406,13 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
   if (!h) return CUP2D_OOM;
   h->opts = o;
   cudaGetDevice(&h->device);
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  // the handle's own stream (assembly, host-buffer solves) at the highest
+  // priority: when a server assembles a new mesh while persistent solves
+  // hold most of the device, its short assembly kernels take the CTA slots
+  // that free up before queued solve work does
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     cup2d_poisson_destroy(h);
     return CUP2D_CUDA_ERROR;

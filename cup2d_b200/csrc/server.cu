@@ -179,6 +179,7 @@ int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
   cup2d_poisson* h = nullptr;
   resident_bytes += need;  // reserved while assembling
   lk.unlock();
+  const Clock::time_point t_asm = Clock::now();
   int st = cup2d_poisson_create(&f, &o, &h);
   if (st == CUP2D_OK) st = cup2d_poisson_set_grid(h, team);
   double* db = nullptr;
@@ -197,6 +198,7 @@ int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
   m.solved = false;
   m.last_used = ++tick;
   ++counters.assemblies;
+  counters.assembly_us += (int64_t)(ms_between(t_asm, Clock::now()) * 1000.0);
   return CUP2D_OK;
 }
 

@@ -329,6 +329,7 @@ typedef struct cup2d_server_counters {
   int64_t submitted, admitted, completed, failed, queued, inflight;
   int64_t resident_meshes, evictions, assemblies;
   int64_t resident_bytes, budget_bytes;
+  int64_t assembly_us;  /* wall time spent making meshes resident (handle creation + assembly), summed */
 } cup2d_server_counters;
 /* x0 = this mesh's last solution when it is still resident (else 0); the
  * request's x is then only written. */
