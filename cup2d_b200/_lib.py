@@ -71,6 +71,13 @@ SIGNATURES = {
                                            C.POINTER(C.c_int32)]),
     "cup2d_poisson_pressure_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.POINTER(SolveStats), C.c_void_p]),
+    "cup2d_poisson_pressure_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cup2d_poisson_pressure_correction": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p]),
+    "cup2d_poisson_pressure_projection": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveStats),
+                                                    C.c_void_p]),
     "cup2d_poisson_set_opts": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts)]),
     "cup2d_poisson_num_cells": (C.c_int64, [C.c_void_p]),
     "cup2d_poisson_set_grid": (C.c_int, [C.c_void_p, C.c_int32]),

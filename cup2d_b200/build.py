@@ -17,8 +17,10 @@ INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libcup2d_poisson.so"
 
-SOURCES = ["assemble.cu", "adapt.cu", "bicgstab.cu", "capi.cu", "noalloc.cu", "precond_tc.cu", "server.cu",
-           "timestep.cu", "spmv_staged.cu", "problems.cpp", "forest.cpp"]
+SOURCES = ["assemble.cu", "adapt.cu", "bicgstab.cu", "capi.cu", "noalloc.cu", "precond_tc.cu", "projection.cu",
+           "server.cu", "timestep.cu", "spmv_staged.cu", "problems.cpp", "forest.cpp"]
+# files whose arithmetic must round like a plain IEEE evaluation (no FMA)
+FILE_FLAGS = {"projection.cu": ["--fmad=false"]}
 HEADERS = ["common.cuh", "kernels.hpp", "spmv.cuh", "handle_view.hpp", "forest.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -49,7 +51,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         o = BUILD / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src, []), "-c", str(s), "-o", str(o)]
             if ptxas_verbose and src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"]
             if verbose:

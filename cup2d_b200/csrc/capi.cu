@@ -184,7 +184,7 @@ struct cup2d_poisson {
   // scan scratch, flag
   DevBuf<uint8_t> ad_state;
   DevBuf<int32_t> ad_mark, ad_rank, ad_scan, ad_flags;
-  DevBuf<double> ps_y, ps_part;  // pressure step: L(pold), weighted-mean partials
+  DevBuf<double> ps_part;  // pressure step: weighted-mean partials
   uint64_t mesh_version = 0;
   bool profiling = false;
   int prof_grid = 0;                // grid of the profiled solves
@@ -667,27 +667,6 @@ int cup2d_poisson_apply(cup2d_poisson* h, const double* d_x, double* d_y, void* 
   return from_cuda(launch_spmv64(h->mesh.view(), d_x, d_y, h->err.p, s));
 }
 
-int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres, double* d_pold,
-                                cup2d_solve_stats* stats, void* stream) {
-  if (!h || !d_tmp || !d_pres || !d_pold || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
-  if (!aligned16(d_tmp) || !aligned16(d_pres) || !aligned16(d_pold)) return CUP2D_INVALID_ARGUMENT;
-  if (d_tmp == d_pres || d_tmp == d_pold || d_pres == d_pold) return CUP2D_INVALID_ARGUMENT;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
-  const int64_t n = h->nb * kBLEN;
-  int st;
-  if ((st = h->ps_y.ensure(n, s)) || (st = h->ps_part.ensure(wmean_partials(h->nb), s))) return st;
-  // POLD = PRES (PressureSingle.cpp:836-846); tmp -= L(pold), PRES = 0 (:847-848, 411-418)
-  if (cudaMemcpyAsync(d_pold, d_pres, sizeof(double) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  if (launch_spmv64(h->mesh.view(), d_pold, h->ps_y.p, h->err.p, s) != cudaSuccess ||
-      launch_rhs_minus_lpold(d_tmp, h->ps_y.p, d_pres, n, s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  // pressureSolver->solve(sim.tmp, sim.pres) (:850)
-  if ((st = cup2d_poisson_solve_device(h, d_tmp, d_pres, stats, stream))) return st;
-  // PRES += POLD - mean(PRES), volume-weighted (:853-879)
-  return from_cuda(launch_add_pold(d_pres, d_pold, h->hblk.p, h->nb, h->ps_part.p, s));
-}
-
 int cup2d_poisson_apply32(cup2d_poisson* h, const float* d_x, float* d_y, void* stream) {
   if (!h || !d_x || !d_y || !aligned16(d_x) || !aligned16(d_y)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
@@ -703,6 +682,8 @@ ForestView forest_view(const cup2d_poisson* h) {
   F.bpdx = h->bpdx;
   F.bpdy = h->bpdy;
   F.L = h->level_max;
+  F.px = h->px;
+  F.py = h->py;
   F.nb = h->nb;
   F.h0 = h->extent / ((double)std::max(h->bpdx, h->bpdy) * 8.0);
   F.level = h->level.p;
@@ -721,6 +702,78 @@ ForestView forest_view(const cup2d_poisson* h) {
 }  // namespace
 
 extern "C" {
+
+namespace {
+
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  if (!a || !b) return false;
+  const char* pa = static_cast<const char*>(a);
+  const char* pb = static_cast<const char*>(b);
+  return pa < pb + nb && pb < pa + na;
+}
+
+}  // namespace
+
+int cup2d_poisson_pressure_rhs(cup2d_poisson* h, double dt, const double* d_vel, const double* d_udef,
+                               const double* d_chi, double* d_pres, double* d_pold, double* d_tmp, void* stream) {
+  if (!h || !d_tmp || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  if (!d_vel && !d_pres) return CUP2D_INVALID_ARGUMENT;
+  if (d_vel && (!d_udef || !d_chi || !(dt > 0.0) || !std::isfinite(dt))) return CUP2D_INVALID_ARGUMENT;
+  if (d_pres && !d_pold) return CUP2D_INVALID_ARGUMENT;
+  const size_t n = (size_t)h->nb * kBLEN * sizeof(double);
+  const void* bufs[6] = {d_tmp, d_pres, d_pold, d_vel, d_udef, d_chi};
+  const size_t size[6] = {n, n, n, 2 * n, 2 * n, n};
+  for (int a = 0; a < 6; ++a)
+    for (int b = a + 1; b < 6; ++b)
+      if (overlaps(bufs[a], size[a], bufs[b], size[b])) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+  const ProjFields f{d_vel, d_vel ? d_udef : nullptr, d_vel ? d_chi : nullptr, d_pres, d_tmp, d_pold};
+  if (launch_pressure_rhs(forest_view(h), h->nbr.p, d_vel ? dt : 1.0, f, s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  // PRES = 0 (PressureSingle.cpp:845): the solve's initial guess
+  if (d_pres && cudaMemsetAsync(d_pres, 0, n, s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
+}
+
+int cup2d_poisson_pressure_correction(cup2d_poisson* h, double dt, const double* d_pres, double* d_vel,
+                                      void* stream) {
+  if (!h || !d_pres || !d_vel || h->nb <= 0 || !(dt > 0.0) || !std::isfinite(dt)) return CUP2D_INVALID_ARGUMENT;
+  const size_t n = (size_t)h->nb * kBLEN * sizeof(double);
+  if (overlaps(d_pres, n, d_vel, 2 * n)) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return from_cuda(launch_pressure_correction(forest_view(h), h->nbr.p, dt, d_pres, d_vel, s));
+}
+
+int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres, double* d_pold,
+                                cup2d_solve_stats* stats, void* stream) {
+  if (!h || !d_tmp || !d_pres || !d_pold || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_tmp) || !aligned16(d_pres) || !aligned16(d_pold)) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+  int st;
+  if ((st = h->ps_part.ensure(wmean_partials(h->nb), s))) return st;
+  // POLD = PRES; TMP -= L(POLD); PRES = 0 (PressureSingle.cpp:836-848, 399-456)
+  if ((st = cup2d_poisson_pressure_rhs(h, 0.0, nullptr, nullptr, nullptr, d_pres, d_pold, d_tmp, stream))) return st;
+  // pressureSolver->solve(sim.tmp, sim.pres) (:850)
+  if ((st = cup2d_poisson_solve_device(h, d_tmp, d_pres, stats, stream))) return st;
+  // PRES += POLD - mean(PRES), volume-weighted (:853-879)
+  return from_cuda(launch_add_pold(d_pres, d_pold, h->hblk.p, h->nb, h->ps_part.p, s));
+}
+
+int cup2d_poisson_pressure_projection(cup2d_poisson* h, double dt, double* d_vel, const double* d_udef,
+                                      const double* d_chi, double* d_pres, double* d_pold, double* d_tmp,
+                                      cup2d_solve_stats* stats, void* stream) {
+  if (!h || !d_vel || !d_udef || !d_chi || !d_pres || !d_pold || !d_tmp || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_tmp) || !aligned16(d_pres) || !aligned16(d_pold)) return CUP2D_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st;
+  if ((st = h->ps_part.ensure(wmean_partials(h->nb), s))) return st;
+  // updatePressureRHS; POLD = PRES, PRES = 0; updatePressureRHS1 (:826-849)
+  if ((st = cup2d_poisson_pressure_rhs(h, dt, d_vel, d_udef, d_chi, d_pres, d_pold, d_tmp, stream))) return st;
+  // solve (:850); PRES += POLD - mean(PRES) (:853-879)
+  if ((st = cup2d_poisson_solve_device(h, d_tmp, d_pres, stats, stream))) return st;
+  if ((st = from_cuda(launch_add_pold(d_pres, d_pold, h->hblk.p, h->nb, h->ps_part.p, s)))) return st;
+  // pressureCorrection(dt) (:881)
+  return cup2d_poisson_pressure_correction(h, dt, d_pres, d_vel, stream);
+}
 
 int cup2d_poisson_rhs_fourier_device(cup2d_poisson* h, int32_t kmax, const double* coef, double* d_b,
                                      void* stream) {

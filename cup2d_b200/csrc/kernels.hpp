@@ -185,6 +185,7 @@ cudaError_t launch_precond32_tc(const float* P32, int64_t nb, const float* p, fl
 // with (bpdx << l) columns).
 struct ForestView {
   int32_t bpdx, bpdy, L;
+  int32_t px, py;  // periodic in x / y
   int64_t nb;
   double h0;  // cell size at level 0
   const int32_t* level;
@@ -234,13 +235,32 @@ int64_t rhs_partials(int64_t nb);  // scratch doubles of launch_rhs_fourier
 // (device, 4 per mode); partial [rhs_partials(nb)] and mean [1] scratch.
 cudaError_t launch_rhs_fourier(const ForestView& F, int kmax, const double* coef, double* b, double* partial,
                                double* mean, cudaStream_t s);
-// Pressure step around the solve (PressureSingle.cpp:831-879): tmp -= y and
-// pres = 0; then pres += pold - (volume-weighted mean of pres), with
-// `partial` scratch of wmean_partials(nb) doubles.
-cudaError_t launch_rhs_minus_lpold(double* tmp, const double* y, double* pres, int64_t n, cudaStream_t s);
+// After the solve of the pressure step (PressureSingle.cpp:853-879):
+// pres += pold - (volume-weighted mean of pres), with `partial` scratch of
+// wmean_partials(nb) doubles.
 int64_t wmean_partials(int64_t nb);
 cudaError_t launch_add_pold(double* pres, const double* pold, const double* hblk, int64_t nb, double* partial,
                             cudaStream_t s);
+// Pressure projection around the solve (projection.cu), one thread per cell.
+// Velocity-like fields hold (u, v) per cell, interleaved, in block-major
+// cell order; scalars one double per cell.
+//   rhs:  tmp = h/(2dt) (central div vel - chi central div udef)  (vel set)
+//         tmp -= 5-point L(pres), pold = pres                       (pres set)
+//   correction: vel += -(dt h/2)(central difference of pres) / h^2
+// Coarse/fine faces take the fine side's ghosts from the coarse block by
+// the quadratic rule of the operator and correct the coarse side's fluxes.
+struct ProjFields {
+  const double* vel;
+  const double* udef;
+  const double* chi;
+  const double* pres;
+  double* tmp;
+  double* pold;
+};
+cudaError_t launch_pressure_rhs(const ForestView& F, const int32_t* nbr, double dt, const ProjFields& f,
+                                cudaStream_t s);
+cudaError_t launch_pressure_correction(const ForestView& F, const int32_t* nbr, double dt, const double* pres,
+                                       double* vel, cudaStream_t s);
 // xd (on D) = xs (on S) carried across a change of forest.
 cudaError_t launch_transfer(const ForestView& S, const double* xs, const ForestView& D, double* xd,
                             cudaStream_t s);

@@ -160,16 +160,6 @@ __global__ void k_transfer(ForestView S, const double* __restrict__ xs, ForestVi
 
 // ------------------------------------------------ pressure step helpers --
 
-// tmp -= y (y = L(pold), the assembled operator applied to the old pressure:
-// updatePressureRHS1, PressureSingle.cpp:411-418), and pres = 0.
-__global__ void k_rhs_minus_lpold(double* __restrict__ tmp, const double* __restrict__ y,
-                                  double* __restrict__ pres, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    tmp[i] -= y[i];
-    pres[i] = 0.0;
-  }
-}
-
 // Per-CTA partial sums of h^2 p and of h^2 over the cells (the volume
 // weights of PressureSingle.cpp:853-868), in a fixed order.
 __global__ void __launch_bounds__(kRhsThreads) k_wsum_partials(const double* __restrict__ p,
@@ -237,11 +227,6 @@ __global__ void k_add_pold(double* __restrict__ pres, const double* __restrict__
 
 }  // namespace
 
-cudaError_t launch_rhs_minus_lpold(double* tmp, const double* y, double* pres, int64_t n, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
-  k_rhs_minus_lpold<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(tmp, y, pres, n);
-  return cudaGetLastError();
-}
 
 int64_t wmean_partials(int64_t nb) { return 2 * ((nb * kBLEN + kRhsThreads - 1) / kRhsThreads) + 1; }
 

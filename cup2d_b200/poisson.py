@@ -139,8 +139,8 @@ class Solver:
     def solve_device(self, b, x, stream=None, stats: bool = True) -> Optional[dict]:
         """Device tensors (torch, float64, contiguous): x holds x0 and receives
         the solution.  With stats=False the call is asynchronous."""
-        _check_dev(b, self.ncells)
-        _check_dev(x, self.ncells)
+        _check_dev(b, self.ncells, F64)
+        _check_dev(x, self.ncells, F64)
         st = L.SolveStats()
         s = _stream_handle(stream)
         L.check(L.lib().cup2d_poisson_solve_device(self._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
@@ -156,12 +156,56 @@ class Solver:
         pold = pres; tmp -= L(pold); pres = solve(tmp); pres += pold - mean.
         Returns the solve's statistics (the call synchronises)."""
         for t in (tmp, pres, pold):
-            _check_dev(t, self.ncells)
+            _check_dev(t, self.ncells, F64)
         st = L.SolveStats()
         L.check(L.lib().cup2d_poisson_pressure_step(self._h, C.c_void_p(tmp.data_ptr()), C.c_void_p(pres.data_ptr()),
                                                      C.c_void_p(pold.data_ptr()), C.byref(st),
                                                      _stream_handle(stream)),
                 "cup2d_poisson_pressure_step")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def pressure_rhs(self, dt: float, vel=None, udef=None, chi=None, pres=None, pold=None, tmp=None,
+                     stream=None) -> None:
+        """What PressureSingle::operator() does before the solve, on device
+        tensors (float64, block-major cells; vel and udef (ncells, 2)):
+        with vel: tmp = updatePressureRHS(vel, udef, chi) at time step dt;
+        with pres: pold = pres, tmp -= updatePressureRHS1(pold), pres = 0.
+        Asynchronous on `stream`."""
+        n = self.ncells
+        if vel is not None:
+            for t, k in ((vel, 2 * n), (udef, 2 * n), (chi, n)):
+                _check_dev(t, k, F64)
+        if pres is not None:
+            _check_dev(pres, n, F64)
+            _check_dev(pold, n, F64)
+        _check_dev(tmp, n, F64)
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731
+        L.check(L.lib().cup2d_poisson_pressure_rhs(self._h, float(dt), ptr(vel), ptr(udef), ptr(chi), ptr(pres),
+                                                    ptr(pold), ptr(tmp), _stream_handle(stream)),
+                "cup2d_poisson_pressure_rhs")
+
+    def pressure_correction(self, dt: float, pres, vel, stream=None) -> None:
+        """PressureSingle::pressureCorrection: vel += -0.5 dt h grad(pres) / h^2
+        (central differences, flux-corrected), in place.  Asynchronous."""
+        _check_dev(pres, self.ncells, F64)
+        _check_dev(vel, 2 * self.ncells, F64)
+        L.check(L.lib().cup2d_poisson_pressure_correction(self._h, float(dt), C.c_void_p(pres.data_ptr()),
+                                                           C.c_void_p(vel.data_ptr()), _stream_handle(stream)),
+                "cup2d_poisson_pressure_correction")
+
+    def pressure_projection(self, dt: float, vel, udef, chi, pres, pold, tmp, stream=None) -> dict:
+        """The pressure projection of PressureSingle::operator() without the
+        obstacle terms: RHS, solve, pres += pold - mean, velocity correction.
+        Returns the solve's statistics (the call synchronises)."""
+        n = self.ncells
+        for t, k in ((vel, 2 * n), (udef, 2 * n), (chi, n), (pres, n), (pold, n), (tmp, n)):
+            _check_dev(t, k, F64)
+        st = L.SolveStats()
+        p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        L.check(L.lib().cup2d_poisson_pressure_projection(self._h, float(dt), p(vel), p(udef), p(chi), p(pres),
+                                                           p(pold), p(tmp), C.byref(st), _stream_handle(stream)),
+                "cup2d_poisson_pressure_projection")
         self.last_stats = st.as_dict()
         return self.last_stats
 
@@ -172,8 +216,8 @@ class Solver:
         allocation can cause).  Scratch lives in one static 16.2 MiB device
         array shared by all calls: at most CUP2D_NOALLOC_MAX_BLOCKS (4096)
         blocks, and calls that overlap on the GPU race."""
-        _check_dev(b, self.ncells)
-        _check_dev(x, self.ncells)
+        _check_dev(b, self.ncells, F64)
+        _check_dev(x, self.ncells, F64)
         st = L.SolveStats()
         L.check(L.lib().cup2d_poisson_solve_device_noalloc(self._h, C.c_void_p(b.data_ptr()),
                                                            C.c_void_p(x.data_ptr()), C.byref(st),
@@ -186,7 +230,9 @@ class Solver:
     def apply(self, x, y, stream=None) -> None:
         """y = A x on device tensors: float64, or float32 (the mixed form's SpMV)."""
         _check_dev(x, self.ncells)
-        _check_dev(y, self.ncells)
+        _check_dev(y, self.ncells, str(x.dtype))
+        if str(x.dtype) not in ("torch.float32", F64):
+            raise ValueError(f"expected float32 or float64 tensors, got {x.dtype}")
         s = _stream_handle(stream)
         fn = L.lib().cup2d_poisson_apply32 if str(x.dtype) == "torch.float32" else L.lib().cup2d_poisson_apply
         L.check(fn(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), s), "cup2d_poisson_apply")
@@ -196,15 +242,15 @@ class Solver:
         forest for Fourier coefficients `coef` (Mesh.rhs_from_coefs on the
         device)."""
         coef = np.ascontiguousarray(coef, dtype=np.float64)
-        _check_dev(b, self.ncells)
+        _check_dev(b, self.ncells, F64)
         L.check(L.lib().cup2d_poisson_rhs_fourier_device(self._h, int(kmax), _pd(coef), C.c_void_p(b.data_ptr()),
                                                          _stream_handle(stream)), "cup2d_poisson_rhs_fourier_device")
 
     def transfer_to(self, dst: "Solver", x_src, x_dst, stream=None) -> None:
         """x_dst (on dst's forest) = x_src (on this forest), e.g. a warm
         start carried across a mesh adaptation."""
-        _check_dev(x_src, self.ncells)
-        _check_dev(x_dst, dst.ncells)
+        _check_dev(x_src, self.ncells, F64)
+        _check_dev(x_dst, dst.ncells, F64)
         L.check(L.lib().cup2d_poisson_transfer(self._h, C.c_void_p(x_src.data_ptr()), dst._h,
                                                C.c_void_p(x_dst.data_ptr()), _stream_handle(stream)),
                 "cup2d_poisson_transfer")
@@ -317,8 +363,8 @@ class BatchSolver:
         if len(bs) != n or len(xs) != n:
             raise ValueError(f"expected {n} right-hand sides and solutions")
         for i in range(n):
-            _check_dev(bs[i], self.ncells(i))
-            _check_dev(xs[i], self.ncells(i))
+            _check_dev(bs[i], self.ncells(i), F64)
+            _check_dev(xs[i], self.ncells(i), F64)
         pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
         px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
         st = (L.SolveStats * n)()
@@ -361,8 +407,8 @@ class BatchSolver:
                 return team, cps
         n = len(self)
         for i in range(n):
-            _check_dev(bs[i], self.ncells(i))
-            _check_dev(xs[i], self.ncells(i))
+            _check_dev(bs[i], self.ncells(i), F64)
+            _check_dev(xs[i], self.ncells(i), F64)
         pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
         px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
         ct = (C.c_int32 * len(teams))(*teams)
@@ -391,8 +437,8 @@ class BatchSolver:
         if len(bs) != n or len(xs) != n:
             raise ValueError(f"expected {n} right-hand sides and solutions")
         for i in range(n):
-            _check_dev(bs[i], self.ncells(i))
-            _check_dev(xs[i], self.ncells(i))
+            _check_dev(bs[i], self.ncells(i), F64)
+            _check_dev(xs[i], self.ncells(i), F64)
         pb = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
         px = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
         L.check(L.lib().cup2d_batch_capture(self._h, pb, px, L.GRAPH_ZERO_X if zero_x else 0), "cup2d_batch_capture")
@@ -552,9 +598,14 @@ def _stream_handle(stream) -> C.c_void_p:
     return C.c_void_p(stream.cuda_stream)
 
 
-def _check_dev(t, n: int) -> None:
+F64 = "torch.float64"
+
+
+def _check_dev(t, n: int, dtype: str | None = None) -> None:
     if not (hasattr(t, "is_cuda") and t.is_cuda and t.is_contiguous() and t.numel() == n):
         raise ValueError(f"expected a contiguous CUDA tensor of {n} elements")
+    if dtype is not None and str(t.dtype) != dtype:
+        raise ValueError(f"expected a {dtype} tensor, got {t.dtype}")
 
 
 def device_pinv() -> np.ndarray:

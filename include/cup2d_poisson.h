@@ -195,8 +195,9 @@ int cup2d_poisson_transfer(const cup2d_poisson* src, const double* d_xsrc, const
  *   pold = pres; tmp -= L(pold); pres = 0            (:836-848, 411-418)
  *   solve L pres = tmp (cup2d_poisson_solve_device)  (:850)
  *   pres += pold - mean(pres), volume-weighted       (:853-879)
- * L is the assembled operator (the same rows updatePressureRHS1 applies with
- * Cubism's ghost cells and flux correction).  On entry d_tmp holds the
+ * L(pold) is updatePressureRHS1's 5-point stencil on block labs with the
+ * coarse/fine flux correction (the kernel of cup2d_poisson_pressure_rhs; in
+ * exact arithmetic the assembled operator).  On entry d_tmp holds the
  * divergence part of the right-hand side (updatePressureRHS) and d_pres the
  * previous pressure; on return d_pres holds the new pressure, d_pold the
  * previous one and d_tmp the right-hand side that was solved.  The three
@@ -205,6 +206,42 @@ int cup2d_poisson_transfer(const cup2d_poisson* src, const double* d_xsrc, const
  * queued on the stream). */
 int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres, double* d_pold,
                                 cup2d_solve_stats* stats, void* stream);
+
+/* The field kernels of the pressure projection (source/Operators/
+ * PressureSingle.cpp), on device buffers in block-major cell order.
+ * Velocity-like fields hold (u, v) per cell, interleaved (Cubism's
+ * VectorBlock layout), scalars one double per cell; each buffer holds the
+ * handle's ncells cells.  Ghost cells follow CUP2D's labs: same-level
+ * neighbours, domain edges (velocities: normal component sign-flipped;
+ * scalars: copied), coarser neighbours by the operator's quadratic
+ * interpolation (ExpAMRSolver.cpp:100-128), and coarse cells next to finer
+ * blocks take the fine side's fluxes (Cubism's flux correction).
+ *
+ * cup2d_poisson_pressure_rhs: everything operator() does before the solve
+ * (:826-849).  With d_vel set (then d_udef and d_chi too):
+ *   tmp = 0.5 h/dt ((u_E - u_W) + (v_N - v_S))
+ *         - 0.5 h/dt chi ((ud_E - ud_W) + (vd_N - vd_S))   (updatePressureRHS)
+ * else d_tmp is read as it is.  With d_pres set (then d_pold too):
+ *   pold = pres; tmp -= (p_W + p_E + p_S + p_N - 4 p)[pold]; pres = 0
+ *                                                       (updatePressureRHS1)
+ * At least one of d_vel, d_pres must be set; tmp, pres, pold, vel, udef and
+ * chi must not overlap.  Asynchronous on `stream`. */
+int cup2d_poisson_pressure_rhs(cup2d_poisson* h, double dt, const double* d_vel, const double* d_udef,
+                               const double* d_chi, double* d_pres, double* d_pold, double* d_tmp, void* stream);
+/* PressureSingle::pressureCorrection (:123-210): with pFac = -0.5 dt h,
+ *   vel += pFac (P_E - P_W, P_N - P_S) / h^2   (flux-corrected at coarse/fine faces).
+ * d_pres and d_vel must not overlap.  Asynchronous on `stream`. */
+int cup2d_poisson_pressure_correction(cup2d_poisson* h, double dt, const double* d_pres, double* d_vel,
+                                      void* stream);
+/* The whole pressure projection of PressureSingle::operator() (:826-882)
+ * without the obstacle terms: cup2d_poisson_pressure_rhs (velocities and
+ * pres), the solve, pres += pold - mean(pres), cup2d_poisson_pressure_correction.
+ * On return d_vel holds the projected velocity, d_pres the new pressure,
+ * d_pold the previous one, d_tmp the right-hand side that was solved.
+ * Statistics as cup2d_poisson_pressure_step. */
+int cup2d_poisson_pressure_projection(cup2d_poisson* h, double dt, double* d_vel, const double* d_udef,
+                                      const double* d_chi, double* d_pres, double* d_pold, double* d_tmp,
+                                      cup2d_solve_stats* stats, void* stream);
 int cup2d_poisson_precond(cup2d_poisson* h, const double* d_p, double* d_z, void* stream);
 /* FP32 P^-1 apply of the mixed form (split-TF32 tensor-core MMA). */
 int cup2d_poisson_precond32(cup2d_poisson* h, const float* d_p, float* d_z, void* stream);

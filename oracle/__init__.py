@@ -60,6 +60,10 @@ def lib() -> C.CDLL:
         L.oracle_bicgstab.argtypes = [C.c_void_p, pf, pf, pf, C.c_double, C.c_double, C.c_int, C.c_int,
                                       C.POINTER(OracleStats)]
         L.oracle_subtract_mean.argtypes = [C.c_int64, pf, pf]
+        L.oracle_pressure_rhs.restype = C.c_int
+        L.oracle_pressure_rhs.argtypes = [C.POINTER(OracleForest), C.c_double, pf, pf, pf, pf, pf, pf]
+        L.oracle_pressure_correction.restype = C.c_int
+        L.oracle_pressure_correction.argtypes = [C.POINTER(OracleForest), C.c_double, pf, pf]
         _lib = L
     return _lib
 
@@ -80,6 +84,52 @@ def pinv() -> np.ndarray:
     P = np.empty(64 * 64, dtype=np.float64)
     lib().oracle_pinv(_pd(P))
     return P.reshape(64, 64)
+
+
+def _forest(mesh):
+    arrs = (np.ascontiguousarray(mesh.level, dtype=np.int32), np.ascontiguousarray(mesh.bx, dtype=np.int32),
+            np.ascontiguousarray(mesh.by, dtype=np.int32))
+    f = OracleForest(mesh.bpdx, mesh.bpdy, mesh.level_max, int(mesh.periodic_x), int(mesh.periodic_y),
+                     float(mesh.extent), mesh.nblocks, *(a.ctypes.data_as(C.POINTER(C.c_int32)) for a in arrs))
+    return f, arrs
+
+
+def _opt(a):
+    return None if a is None else _pd(a)
+
+
+def pressure_rhs(mesh, dt: float, vel=None, udef=None, chi=None, pres=None, tmp=None):
+    """PressureSingle.cpp:826-849 before the solve (oracle/projection.cpp).
+
+    vel/udef: (ncells, 2) velocities, chi: (ncells,).  Returns (tmp, pold):
+    tmp = updatePressureRHS of the velocities (when vel is given, else the
+    given tmp), minus updatePressureRHS1 of pres (when pres is given), and
+    pold = pres."""
+    n = mesh.ncells
+    f, keep = _forest(mesh)
+    out = np.zeros(n) if tmp is None else np.array(tmp, dtype=np.float64, copy=True)
+    vel = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).reshape(n, 2)
+    udef = None if udef is None else np.ascontiguousarray(udef, dtype=np.float64).reshape(n, 2)
+    chi = None if chi is None else np.ascontiguousarray(chi, dtype=np.float64)
+    pres = None if pres is None else np.ascontiguousarray(pres, dtype=np.float64)
+    pold = None if pres is None else np.empty(n)
+    if lib().oracle_pressure_rhs(C.byref(f), float(dt), _opt(vel), _opt(udef), _opt(chi), _opt(pres), _pd(out),
+                                 _opt(pold)) != 0:
+        raise ValueError("oracle: malformed forest")
+    del keep
+    return out, pold
+
+
+def pressure_correction(mesh, dt: float, pres, vel):
+    """PressureSingle::pressureCorrection: returns vel + tmpV / h^2."""
+    n = mesh.ncells
+    f, keep = _forest(mesh)
+    pres = np.ascontiguousarray(pres, dtype=np.float64)
+    out = np.array(vel, dtype=np.float64, copy=True).reshape(n, 2)
+    if lib().oracle_pressure_correction(C.byref(f), float(dt), _pd(pres), _pd(out)) != 0:
+        raise ValueError("oracle: malformed forest")
+    del keep
+    return out
 
 
 class Matrix:

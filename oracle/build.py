@@ -10,14 +10,14 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SRC = HERE / "oracle.cpp"
+SRCS = [HERE / "oracle.cpp", HERE / "projection.cpp"]
 LIB = HERE / "liboracle.so"
 
 
 def build(force: bool = False) -> Path:
-    if force or not LIB.exists() or SRC.stat().st_mtime > LIB.stat().st_mtime:
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in SRCS):
         cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-               str(SRC), "-o", str(LIB)]
+               *map(str, SRCS), "-o", str(LIB)]
         subprocess.run(cmd, check=True)
     return LIB
 

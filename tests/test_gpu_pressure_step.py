@@ -4,8 +4,11 @@ PressureSingle.cpp:831-879) built on the oracle:
 
   pold = pres; tmp -= L(pold); pres = 0; solve; pres += pold - mean(pres)
 
-with L the assembled operator (the oracle's, which is the reference's) and
-the volume-weighted mean of :853-868.
+with the volume-weighted mean of :853-868.  The device's L(pold) is
+updatePressureRHS1's flux-corrected 5-point stencil, which equals the
+assembled operator (the oracle's, which is the reference's) to rounding; it
+is compared with the assembled operator's product here and bit for bit with
+the oracle's restatement of updatePressureRHS1 in test_gpu_projection.py.
 """
 import numpy as np
 import pytest
