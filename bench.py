@@ -214,6 +214,39 @@ def spmv_leg(dev, stream, steps: int = 20, warmup: int = 5) -> dict:
                          "achieved": by / (t * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": by / (t * 1e-3) / 1e9 / peak, "peak_kind": kind,
                          "flops_tensor_tflops": 3 * 2 * 64 * n / (t * 1e-3) / 1e12}
+        del p32, z32, x, y
+        # the pressure projection's field kernels on the same forest:
+        # updatePressureRHS + updatePressureRHS1 (read vel, udef 16 B, chi,
+        # pres 8 B; write tmp, pold 8 B; pres = 0 8 B) and pressureCorrection
+        # (read pres 8 B, vel 16 B; write vel 16 B)
+        g = torch.Generator(device=dev).manual_seed(3)
+        vel = torch.randn(2 * n, dtype=torch.float64, device=dev, generator=g)
+        udef = torch.randn(2 * n, dtype=torch.float64, device=dev, generator=g)
+        chi = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+        pres = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+        pres0 = pres.clone()
+        tmp = torch.empty_like(pres)
+        pold = torch.empty_like(pres)
+        for name, by in (("pressure_rhs", 64.0 * n), ("pressure_correction", 40.0 * n)):
+            ms = []
+            for i in range(warmup + steps):
+                if name == "pressure_rhs":
+                    pres.copy_(pres0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if name == "pressure_rhs":
+                    h.pressure_rhs(0.01, vel, udef, chi, pres, pold, tmp, stream=stream)
+                else:
+                    h.pressure_correction(0.01, pres0, vel, stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                if i >= warmup:
+                    ms.append(e0.elapsed_time(e1))
+            t = statistics.median(ms)
+            out[name] = {"kernel": "k_" + name + (" + memset(pres)" if name == "pressure_rhs" else ""), "ms": t,
+                         "bytes": by, "achieved": by / (t * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": by / (t * 1e-3) / 1e9 / peak, "peak_kind": kind}
     return out
 
 

@@ -31,7 +31,8 @@ class Forest(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("tol_abs", C.c_double), ("tol_rel", C.c_double), ("max_restarts", C.c_int32),
                 ("max_iter", C.c_int32), ("precision", C.c_int32), ("subtract_mean", C.c_int32),
-                ("reliable_delta", C.c_double), ("timeout_ms", C.c_int32), ("reliable_restart", C.c_int32)]
+                ("reliable_delta", C.c_double), ("timeout_ms", C.c_int32), ("reliable_restart", C.c_int32),
+                ("mean_constraint", C.c_int32)]
 
 
 class ServerCounters(C.Structure):

@@ -217,6 +217,14 @@ __global__ void k_classify(ForestDev F, int32_t* __restrict__ nbr, unsigned long
   hblk[b] = h0 / (double)(1ll << l);
 }
 
+// The leaf at the domain's (0, 0) corner: the block whose index is (0, 0) at
+// its level (ExpAMRSolver.cpp:251-256 places bMeanConstraint's row there).
+__global__ void k_origin(ForestDev F, int* __restrict__ out) {
+  int32_t b = -1;
+  for (int l = 0; l < F.L && b < 0; ++l) b = F.leaf(l, 0, 0);
+  *out = b;
+}
+
 // ------------------------------------------------------------- scans ------
 
 // Exclusive scan of int32 counts into int32 offsets (out[n] = total), in
@@ -527,15 +535,17 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   if (cudaMemsetAsync(out.err, 0, sizeof(int), s) != cudaSuccess) return CUP2D_CUDA_ERROR;
   k_fill_tables<<<g, 256, 0, s>>>(F, out.table, out.err);
   k_classify<<<g, 256, 0, s>>>(F, out.nbr, out.xmask, out.xcount, out.hblk, in.h0, out.err);
+  k_origin<<<1, 1, 0, s>>>(F, out.err + 1);
   launch_exclusive_scan(out.xcount, nb, out.xbase, out.scan_tmp, s);
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
   int32_t hR = 0;
-  int herr = 0;
+  int herr[2] = {0, -1};
   if (cudaMemcpyAsync(&hR, out.xbase + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(&herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(herr, out.err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
-  if (herr != 0) return CUP2D_BAD_MESH;
+  if (herr[0] != 0 || herr[1] < 0) return CUP2D_BAD_MESH;
+  out.origin = herr[1];
   out.R = hR;
   int st = out.alloc_rows(out.ctx, hR);
   if (st != CUP2D_OK) return st;
@@ -549,10 +559,10 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
   int32_t hnnz = 0;
   if (cudaMemcpyAsync(&hnnz, out.xptr + hR, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(&herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
-  if (herr != 0) return CUP2D_BAD_MESH;
+  if (herr[0] != 0) return CUP2D_BAD_MESH;
   out.nnz = hnnz;
   st = out.alloc_nnz(out.ctx, hnnz);
   if (st != CUP2D_OK) return st;
@@ -562,10 +572,10 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
     launch_convert_f64_f32(out.xval, out.xval32, hnnz, s);
   }
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
-  if (cudaMemcpyAsync(&herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+  if (cudaMemcpyAsync(herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
-  return herr != 0 ? CUP2D_BAD_MESH : CUP2D_OK;
+  return herr[0] != 0 ? CUP2D_BAD_MESH : CUP2D_OK;
 }
 
 int64_t leaf_table_entries(int bpdx, int bpdy, int level_max) {

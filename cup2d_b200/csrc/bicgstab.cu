@@ -67,9 +67,14 @@ enum : int {
   Q_RMAX = 6,   // pass E: |r|_inf, (rhat,r), |r|^2, |rhat|^2
   Q_HX = 10,    // mean removal: sum h^2 x, sum h^2
   Q_RU = 12,    // true residual: |r64|_inf, (rhat,r), |r|^2, |rhat|^2, |r32|_inf
-  Q_SUMB = 17   // sum b
+  Q_SUMB = 17,  // sum b
+  // single solves with the mean constraint (kRedQMean slots)
+  Q_MB = 20,    // pass B: (rhat,nu), sum h^2 z, rhat_m nu_m, rhat_m
+  Q_MD = 24,    // pass D: (t,s), (t,t), sum h^2 z2, t_m s_m, t_m t_m, s_m
+  Q_MX = 30     // sum h^2 x0
 };
 static_assert(Q_SUMB + 1 <= kRedQ, "reduction slots");
+static_assert(Q_MX + 1 <= kRedQMean, "reduction slots (mean constraint)");
 
 // Shared memory of the solve kernels, per precision T of the Krylov vectors:
 // P^-1, the P^-1 staging tiles, the staged SpMV rings and the reduction
@@ -298,6 +303,24 @@ struct Pinv<float> {
 
 // ----------------------------------------------------- iteration core -----
 
+// bMeanConstraint (BiCGSTAB.cu:393-410, ExpAMRSolver.cpp:251-256, 340-346):
+// the SpMV's row `mean_row` is replaced by sum_i h_i^2 v_i over the operand v
+// and the right-hand side reads 0 there.  Each CTA adds the h^2-weighted sum
+// of its own blocks of v (this thread's share).
+template <class T>
+__device__ __forceinline__ double hsum_part(const MeshView& M, const T* __restrict__ v, int b0, int b1) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double a = 0.0;
+  for (int blk = b0 + w; blk < b1; blk += kWarps) {
+    const double hb = __ldg(M.hblk + blk);
+    const int o = blk * kBLEN;
+    a += ((double)__ldcg(v + o + lane) + (double)__ldcg(v + o + lane + 32)) * (hb * hb);
+  }
+  return a;
+}
+
+__device__ __forceinline__ bool owns_row(int row, int b0, int b1) { return row >= b0 * kBLEN && row < b1 * kBLEN; }
+
 struct IterState {
   double rho, nr, nrh;  // (rhat,r), |r|^2, |rhat|^2 of the current residual
   double err_init;      // L-inf norm the relative test divides by
@@ -449,11 +472,13 @@ struct MixedCtx {  // what the reliable update needs
 // Runs BiCGSTABSolver::main's loop from a prepared state (r, rhat = r,
 // st.rho/nr/nrh/err_init set, p = nu = 0 implied).  T is the Krylov type,
 // X the solution type; RU enables the mixed form's true-residual
-// replacement.  Returns false if a barrier gave up.
-template <class T, bool RU>
+// replacement; MC the mean constraint (FP64 only).  Returns false if a
+// barrier gave up.
+template <class T, bool RU, bool MC>
 __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, const Problem<T>& V,
                               double* __restrict__ red, int b0, int b1, int r0, int r1, const SolveParams& sp,
                               const MixedCtx& mx, IterState& st) {
+  static_assert(!(MC && RU), "the mean constraint runs in the FP64 form only");
   using X = double;
   const MeshView& M = V.M;
   constexpr int TB = Pinv<T>::kTile;
@@ -531,12 +556,34 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
     {
       EpiRhNu<T> epi{V.rh, V.nu, 0.0};
       spmv_range_staged<T>(M, V.z, V.rh, b0, b1, r0, r1, epi, spmv_stage(sm));
-      const double v[1] = {epi.acc};
-      cta_partials<1>(sm, v, 0u, red, Q_RHNU);
+      if constexpr (MC) {
+        // the mean row's own product and rhat, to swap in sum h^2 z below
+        double v[4] = {epi.acc, hsum_part(M, V.z, b0, b1), 0.0, 0.0};
+        __syncthreads();
+        if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) {
+          const T y = __ldcg(V.nu + sp.mean_row), rv = __ldcg(V.rh + sp.mean_row);
+          v[2] = dprod(rv, y);
+          v[3] = (double)rv;
+        }
+        cta_partials<4>(sm, v, 0u, red, Q_MB);
+      } else {
+        const double v[1] = {epi.acc};
+        cta_partials<1>(sm, v, 0u, red, Q_RHNU);
+      }
     }
     if (!B.sync(&sm.flag, 2)) return false;
-    grid_reduce<1>(sm, 0u, red, Q_RHNU);
-    alpha = rho / (sm.gres[0] + eps);
+    double rhnu;
+    if constexpr (MC) {
+      grid_reduce<4>(sm, 0u, red, Q_MB);
+      const T m = (T)sm.gres[1];
+      rhnu = (sm.gres[0] - sm.gres[2]) + sm.gres[3] * (double)m;
+      if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) V.nu[sp.mean_row] = m;
+      __syncthreads();
+    } else {
+      grid_reduce<1>(sm, 0u, red, Q_RHNU);
+      rhnu = sm.gres[0];
+    }
+    alpha = rho / (rhnu + eps);
     const T ta = (T)alpha;
     // pass C: s = r - alpha nu (in place of r); z2 = P^-1 s
     {
@@ -577,12 +624,34 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
     {
       EpiTS<T> epi{V.r, V.t, 0.0, 0.0};
       spmv_range_staged<T>(M, V.z2, V.r, b0, b1, r0, r1, epi, spmv_stage(sm));
-      const double v[2] = {epi.ts, epi.tt};
-      cta_partials<2>(sm, v, 0u, red, Q_TS);
+      if constexpr (MC) {
+        double v[6] = {epi.ts, epi.tt, hsum_part(M, V.z2, b0, b1), 0.0, 0.0, 0.0};
+        __syncthreads();
+        if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) {
+          const T y = __ldcg(V.t + sp.mean_row), sv = __ldcg(V.r + sp.mean_row);
+          v[3] = dprod(y, sv);
+          v[4] = dprod(y, y);
+          v[5] = (double)sv;
+        }
+        cta_partials<6>(sm, v, 0u, red, Q_MD);
+      } else {
+        const double v[2] = {epi.ts, epi.tt};
+        cta_partials<2>(sm, v, 0u, red, Q_TS);
+      }
     }
     if (!B.sync(&sm.flag, 4)) return false;
-    grid_reduce<2>(sm, 0u, red, Q_TS);
-    omega = sm.gres[0] / (sm.gres[1] + eps);
+    if constexpr (MC) {
+      grid_reduce<6>(sm, 0u, red, Q_MD);
+      const T m = (T)sm.gres[2];
+      const double ts = (sm.gres[0] - sm.gres[3]) + sm.gres[5] * (double)m;
+      const double tt = (sm.gres[1] - sm.gres[4]) + dprod(m, m);
+      omega = ts / (tt + eps);
+      if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) V.t[sp.mean_row] = m;
+      __syncthreads();
+    } else {
+      grid_reduce<2>(sm, 0u, red, Q_TS);
+      omega = sm.gres[0] / (sm.gres[1] + eps);
+    }
     const T to = (T)omega;
     // pass E: x += alpha z, then x += omega z2 (the reference's two axpys,
     // fused into one pass); r = s - omega t; norms.  The best iterate is
@@ -746,16 +815,28 @@ __device__ __forceinline__ void write_stats(const SM& sm, DevStats* stats, const
 // Plain FP64 solve of one problem by the team: BiCGSTABSolver::main
 // (BiCGSTAB.cu:412-620) and the mean removal (ExpAMRSolver.cpp:383-415).
 // [b0,b1) is this CTA's block range, [r0,r1) its explicit rows.
+// MC: the mean constraint (sp.mean_row).
+template <bool MC>
 __device__ bool solve_fp64(Smem<double>& sm, GridBarrier& B, const Pinv<double>& pin, const Problem64& pr,
                            const SolveParams& sp, double* __restrict__ red, int b0, int b1, int r0,
                            int r1) {
   const MeshView& M = pr.M;
+  double x0sum = 0.0;  // MC: sum h^2 x0, the mean row of A x0
+  if constexpr (MC) {
+    const double v[1] = {hsum_part(M, pr.x, b0, b1)};
+    cta_partials<1>(sm, v, 0u, red, Q_MX);
+    if (!B.sync(&sm.flag, 9)) return false;
+    grid_reduce<1>(sm, 0u, red, Q_MX);
+    x0sum = sm.gres[0];
+  }
   // r = b - A x0, rhat = r, |A x0|_inf, |r0|_inf (BiCGSTAB.cu:430-465)
   {
     struct Epi {
       const double* b;
       double* r;
       double* rh;
+      int mrow;
+      double msum;
       double v[3];
       struct Pre {
         double b[2];
@@ -777,19 +858,23 @@ __device__ bool solve_fp64(Smem<double>& sm, GridBarrier& B, const Pinv<double>&
         v[2] += rv * rv;
         return rv;
       }
+      // the mean row: (A x0) reads sum h^2 x0, b reads 0 (getVec, ExpAMRSolver.cpp:340-346)
+      __device__ __forceinline__ double accm(int i, double y, double bi) {
+        return (MC && i == mrow) ? acc(msum, 0.0) : acc(y, bi);
+      }
       __device__ __forceinline__ void vec(int i0, const double (&y)[2], const Pre& p) {
         double rr[2];
-        rr[0] = acc(y[0], p.b[0]);
-        rr[1] = acc(y[1], p.b[1]);
+        rr[0] = accm(i0, y[0], p.b[0]);
+        rr[1] = accm(i0 + 1, y[1], p.b[1]);
         stv<2>(r + i0, rr);
         stv<2>(rh + i0, rr);
       }
       __device__ __forceinline__ void one(int i, double y, const Pre& p, int j) {
-        const double rv = acc(y, p.b[j]);
+        const double rv = accm(i, y, p.b[j]);
         r[i] = rv;
         rh[i] = rv;
       }
-    } epi{pr.b, pr.r, pr.rh, {0.0, 0.0, 0.0}};
+    } epi{pr.b, pr.r, pr.rh, sp.mean_row, x0sum, {0.0, 0.0, 0.0}};
     spmv_range<double>(M, pr.x, b0, b1, r0, r1, epi, spmv_row(sm));
     cta_partials<3>(sm, epi.v, 0x3u, red, Q_INIT);
   }
@@ -807,7 +892,7 @@ __device__ bool solve_fp64(Smem<double>& sm, GridBarrier& B, const Pinv<double>&
   st.best_is_x = true;
   st.status = CUP2D_NOT_CONVERGED;
   const MixedCtx none{};
-  if (!bicgstab_loop<double, false>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, none, st))
+  if (!bicgstab_loop<double, false, MC>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, none, st))
     return false;
   take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
   if (sp.subtract_mean && !subtract_mean(sm, B, M, pr.x, red, b0, b1)) return false;
@@ -856,7 +941,7 @@ __device__ bool solve_mixed(Smem<float>& sm, GridBarrier& B, const Pinv<float>& 
   const bool done0 = st.err_true <= sp.tol_abs || st.err_true == 0.0;
   if (done0) {
     st.status = CUP2D_OK;
-  } else if (!bicgstab_loop<float, true>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, mx, st)) {
+  } else if (!bicgstab_loop<float, true, false>(sm, B, pin, pr, red, b0, b1, r0, r1, sp, mx, st)) {
     return false;
   }
   take_best(st.best_is_x, pr.x, pr.xo, b0, b1);
@@ -893,7 +978,25 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(c
   Pinv<double> pin;
   pin.load(sm.P, S.P, nullptr);
   __syncthreads();
-  solve_fp64(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
+  solve_fp64<false>(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
+}
+
+// With bMeanConstraint: the same solve on the system whose row S.sp.mean_row
+// is sum h^2 x = 0.
+__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm)
+    k_bicgstab64_mean(const __grid_constant__ SolveArgs64 S) {
+  Smem<double>& sm = solve_smem<double>();
+  const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
+  if (threadIdx.x == 0) {
+    sm.team_rank = blockIdx.x;
+    sm.team_size = gridDim.x;
+  }
+  Pinv<double> pin;
+  pin.load(sm.P, S.P, nullptr);
+  __syncthreads();
+  solve_fp64<true>(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
 }
 
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mixed(const __grid_constant__ SolveArgsMixed S) {
@@ -910,6 +1013,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   __syncthreads();
   solve_mixed(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
 }
+
 
 // ========================================================= batches ========
 //
@@ -958,7 +1062,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
       const Problem64& pr = A.p64[p];
       const int b0 = share(pr.M.nb, rank, team), b1 = share(pr.M.nb, rank + 1, team);
       const int r0 = share(pr.M.R, rank, team), r1 = share(pr.M.R, rank + 1, team);
-      ok = solve_fp64(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
+      ok = solve_fp64<false>(sm, B, pin, pr, A.sp, red, b0, b1, r0, r1);
     }
     if (!ok) return;
     if (rank == 0 && threadIdx.x == 0) {
@@ -980,8 +1084,10 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_bat
 // ------------------------------------------------------------ launch -----
 
 namespace {
-const void* const kSolveFns[4] = {(const void*)k_bicgstab64, (const void*)k_bicgstab_mixed,
-                                  (const void*)k_bicgstab_batch64, (const void*)k_bicgstab_batch_mixed};
+constexpr int kNumSolveFns = 5;
+const void* const kSolveFns[kNumSolveFns] = {(const void*)k_bicgstab64, (const void*)k_bicgstab_mixed,
+                                             (const void*)k_bicgstab_batch64, (const void*)k_bicgstab_batch_mixed,
+                                             (const void*)k_bicgstab64_mean};
 
 size_t smem_bytes(const void* fn) {
   return (fn == kSolveFns[1] || fn == kSolveFns[3]) ? sizeof(Smem<float>) : sizeof(Smem<double>);
@@ -997,7 +1103,7 @@ cudaError_t allow_smem(const void* fn) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   int k = 0;
-  while (k < 4 && kSolveFns[k] != fn) ++k;
+  while (k < kNumSolveFns && kSolveFns[k] != fn) ++k;
   const unsigned bit = 1u << k;
   if (dev >= 0 && dev < 64 && (__atomic_load_n(&done[dev], __ATOMIC_ACQUIRE) & bit)) return cudaSuccess;
   const size_t bytes = smem_bytes(fn);
@@ -1030,15 +1136,18 @@ int coop_grid(const void* fn, int device) {
 int max_coop_grid_fp64(int device) { return coop_grid((const void*)k_bicgstab64, device); }
 int max_coop_grid_mixed(int device) { return coop_grid((const void*)k_bicgstab_mixed, device); }
 
+int max_coop_grid_mean(int device) { return coop_grid((const void*)k_bicgstab64_mean, device); }
+
 cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s) {
   void* args[] = {const_cast<SolveArgs64*>(&a)};
-  if (cudaError_t e = allow_smem((const void*)k_bicgstab64)) return e;
-  return cudaLaunchCooperativeKernel((const void*)k_bicgstab64, dim3(grid), dim3(kSolveThreads), args,
-                                     sizeof(Smem<double>), s);
+  const void* fn = a.sp.mean_row >= 0 ? (const void*)k_bicgstab64_mean : (const void*)k_bicgstab64;
+  if (cudaError_t e = allow_smem(fn)) return e;
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolveThreads), args, sizeof(Smem<double>), s);
 }
 
 cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s) {
   void* args[] = {const_cast<SolveArgsMixed*>(&a)};
+  if (a.sp.mean_row >= 0) return cudaErrorInvalidValue;  // FP64 only
   if (cudaError_t e = allow_smem((const void*)k_bicgstab_mixed)) return e;
   return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args,
                                      sizeof(Smem<float>), s);

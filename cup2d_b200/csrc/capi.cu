@@ -139,6 +139,9 @@ int validate_opts(const cup2d_solve_opts& o) {
   if (o.reliable_restart != 0 && o.reliable_restart != 1) return CUP2D_INVALID_ARGUMENT;
   if (o.precision != CUP2D_PREC_FP64 && o.precision != CUP2D_PREC_MIXED) return CUP2D_INVALID_ARGUMENT;
   if (o.timeout_ms <= 0) return CUP2D_INVALID_ARGUMENT;
+  // the mean constraint is the FP64 drop-in's (the mixed form's FP32 sweeps
+  // derail on the constrained system)
+  if (o.mean_constraint && o.precision != CUP2D_PREC_FP64) return CUP2D_INVALID_ARGUMENT;
   return CUP2D_OK;
 }
 
@@ -191,6 +194,7 @@ struct cup2d_poisson {
   DevStats* hstats = nullptr;  // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int grid64 = 0, gridmx = 0;      // max co-resident grids
+  int grid64m = 0;                 // ... of the mean-constraint kernel
   int grid_override = 0;           // tuner / user choice (0 = heuristic)
   int blocks_per_cta = 8;          // heuristic target
 
@@ -250,7 +254,7 @@ int assemble_blocks(cup2d_poisson* h, const cup2d_forest* f, int64_t nb) {
   const int64_t entries = leaf_table_entries(f->bpdx, f->bpdy, f->level_max);
   if ((st = h->table.ensure(entries)) || (st = h->nbr.ensure(4 * nb)) || (st = h->xmask.ensure(nb)) ||
       (st = h->xcount.ensure(nb)) || (st = h->xbase.ensure(nb + 1)) || (st = h->hblk.ensure(nb)) ||
-      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(1)))
+      (st = h->scan_tmp.ensure(scan_temp_ints(n) + 2)) || (st = h->err.ensure(2)))
     return st;
   // the best-iterate copy; the Krylov vectors of a precision are allocated
   // by its first solve
@@ -305,7 +309,7 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
 int ensure_scratch(cup2d_poisson* h) {
   int st;
   const int g = std::max(h->grid64, h->gridmx);
-  if ((st = h->red.ensure((int64_t)kRedQ * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
+  if ((st = h->red.ensure((int64_t)kRedQMean * std::max(g, 1))) || (st = h->bar.ensure(1)) ||
       (st = h->abort_flag.ensure(1)) || (st = h->dstats.ensure(1)))
     return st;
   return CUP2D_OK;
@@ -376,6 +380,7 @@ void cup2d_default_opts(cup2d_solve_opts* o) {
   o->reliable_delta = 0.5;
   o->reliable_restart = 1;
   o->timeout_ms = 20000;
+  o->mean_constraint = 0;
 }
 
 int cup2d_pinv(double* P_out) {
@@ -419,6 +424,7 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
   }
   h->grid64 = max_coop_grid_fp64(h->device);
   h->gridmx = max_coop_grid_mixed(h->device);
+  h->grid64m = std::min(h->grid64, max_coop_grid_mean(h->device));
   if (h->grid64 <= 0 || h->gridmx <= 0) {
     cup2d_poisson_destroy(h);
     return CUP2D_CUDA_ERROR;
@@ -577,7 +583,11 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     return CUP2D_CUDA_ERROR;
   const unsigned long long tns = (unsigned long long)o.timeout_ms * 1000000ull;
   // the barrier counter counts arrivals of the whole solve in 32 bits
-  const int grid = o.precision == CUP2D_PREC_MIXED ? h->grid_for(h->gridmx) : h->grid_for(h->grid64);
+  // bMeanConstraint: row of cell (0,0) of the leaf at the domain's corner
+  const int mean_row = o.mean_constraint ? (int)h->mesh.origin * kBLEN : -1;
+  const bool mixed = o.precision == CUP2D_PREC_MIXED;
+  const int grid = h->grid_for(mixed ? h->gridmx : mean_row >= 0 ? h->grid64m : h->grid64);
+  if (grid <= 0) return CUP2D_CUDA_ERROR;
   const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;
   unsigned long long* prof = nullptr;
@@ -611,7 +621,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
     a.sp = SolveParams{o.tol_abs, o.tol_rel, o.reliable_delta, o.max_restarts, o.max_iter, o.subtract_mean,
-                       o.reliable_restart};
+                       o.reliable_restart, mean_row};
     a.timeout_ns = tns;
     a.prof = prof;
     e = launch_bicgstab_mixed(a, grid, s);
@@ -624,7 +634,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.red = h->red.p;
     a.bar = h->bar.p;
     a.abort_flag = h->abort_flag.p;
-    a.sp = SolveParams{o.tol_abs, o.tol_rel, 0.0, o.max_restarts, o.max_iter, o.subtract_mean, 0};
+    a.sp = SolveParams{o.tol_abs, o.tol_rel, 0.0, o.max_restarts, o.max_iter, o.subtract_mean, 0, mean_row};
     a.timeout_ns = tns;
     a.prof = prof;
     e = launch_bicgstab64(a, grid, s);
@@ -1032,6 +1042,7 @@ int cup2d_batch_create(int32_t n, const cup2d_forest* forests, const cup2d_solve
   if (opts) o = *opts;
   int st = validate_opts(o);
   if (st) return st;
+  if (o.mean_constraint) return CUP2D_INVALID_ARGUMENT;  // single solves only
   for (int32_t i = 0; i < n; ++i)
     if ((st = check_forest(&forests[i]))) return st;
   int ndev = 0;
@@ -1105,6 +1116,7 @@ int cup2d_batch_set_opts(cup2d_batch* B, const cup2d_solve_opts* opts) {
   if (!B || !opts) return CUP2D_INVALID_ARGUMENT;
   int st = validate_opts(*opts);
   if (st) return st;
+  if (opts->mean_constraint) return CUP2D_INVALID_ARGUMENT;  // single solves only
   B->opts = *opts;
   return CUP2D_OK;
 }

@@ -34,7 +34,8 @@ struct DeviceMesh {
   int32_t* xbase = nullptr;       // [nb+1]
   double* hblk = nullptr;         // [nb]
   int32_t* scan_tmp = nullptr;
-  int* err = nullptr;
+  int* err = nullptr;             // [2]: error flag, then the origin block
+  int32_t origin = -1;            // leaf at the domain's (0, 0) corner (read back)
   int64_t R = 0, nnz = 0;
   int32_t* rowlen = nullptr;      // [R]
   int32_t* rowcell = nullptr;     // [R]
@@ -84,7 +85,8 @@ struct DevStats {
   unsigned long long t_begin, t_end;  // batch: globaltimer ns when the team took / finished the problem
 };
 
-constexpr int kRedQ = 20;  // reduction quantities per CTA
+constexpr int kRedQ = 20;      // reduction quantities per CTA
+constexpr int kRedQMean = 31;  // ... of the FP64 single solve with the mean constraint
 
 // One problem of a solve: its operator, right-hand side, FP64 solution and
 // best iterate, and the Krylov vectors (type T: FP64, or FP32 for the mixed
@@ -110,6 +112,10 @@ using ProblemMixed = Problem<float>;
 struct SolveParams {
   double tol_abs, tol_rel, reliable_delta;
   int max_restarts, max_iter, subtract_mean, reliable_restart;
+  // bMeanConstraint: the cell whose equation is replaced by sum(h^2 x) = 0
+  // (its right-hand side read as 0); -1 when off.  Read only by
+  // k_bicgstab64_mean.
+  int mean_row = -1;
 };
 
 // A single solve.  The kernels take these as __grid_constant__ parameters
@@ -166,8 +172,11 @@ constexpr int kSolveCtasPerSm = CUP2D_CTAS_PER_SM;
 // Largest co-resident grid of the persistent kernels on this device.
 int max_coop_grid_fp64(int device);
 int max_coop_grid_mixed(int device);
+// With a.sp.mean_row >= 0 the FP64 launch runs the mean-constraint variant
+// (its red holds kRedQMean quantities per CTA); the mixed form has none.
 cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s);
 cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s);
+int max_coop_grid_mean(int device);
 int max_coop_grid_batch(int device, bool mixed);
 cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s);
 

@@ -111,6 +111,7 @@ extern "C" int cup2d_poisson_solve_device_noalloc(cup2d_poisson* h, const double
   int st = noalloc_scratch_base(current, &base);
   if (st != CUP2D_OK) return st;
   const cup2d_solve_opts& o = v.opts;
+  if (o.mean_constraint) return CUP2D_INVALID_ARGUMENT;  // the plain FP64 kernel only
   const int grid = std::max(1, std::min(v.grid, kNoAllocMaxGrid));
   const uint64_t arrivals = ((uint64_t)o.max_iter * 7 + 16) * (uint64_t)grid;
   if (arrivals >= (1ull << 32)) return CUP2D_INVALID_ARGUMENT;

@@ -35,7 +35,8 @@ def default_opts() -> L.SolveOpts:
 
 
 def make_opts(tol_abs=0.0, tol_rel=1e-8, max_restarts=100, max_iter=1000, precision="fp64",
-              subtract_mean=True, reliable_delta=0.5, reliable_restart=True, timeout_ms=20000) -> L.SolveOpts:
+              subtract_mean=True, reliable_delta=0.5, reliable_restart=True, timeout_ms=20000,
+              mean_constraint=0) -> L.SolveOpts:
     o = default_opts()
     o.tol_abs = tol_abs
     o.tol_rel = tol_rel
@@ -47,6 +48,7 @@ def make_opts(tol_abs=0.0, tol_rel=1e-8, max_restarts=100, max_iter=1000, precis
     o.reliable_delta = reliable_delta
     o.reliable_restart = int(bool(reliable_restart))
     o.timeout_ms = timeout_ms
+    o.mean_constraint = int(mean_constraint)
     return o
 
 
@@ -663,8 +665,6 @@ class ExpAMRSolver(PoissonSolver):
     removed (:383-415)."""
 
     def __init__(self, sim: SimulationData):
-        if sim.bMeanConstraint:
-            raise NotImplementedError("bMeanConstraint != 0 is not supported by this solver")
         self.sim = sim
         self.solver = Solver(sim.mesh, self._opts())
         sim.UpdateFluxCorrection = False
@@ -674,7 +674,7 @@ class ExpAMRSolver(PoissonSolver):
         early = s.step < 10
         return make_opts(tol_abs=0.0 if early else s.PoissonTol, tol_rel=0.0 if early else s.PoissonTolRel,
                          max_restarts=100 if early else s.maxPoissonRestarts, max_iter=s.maxPoissonIterations,
-                         precision=s.precision)
+                         precision=s.precision, mean_constraint=s.bMeanConstraint)
 
     def solve(self, input: ScalarGrid, output: ScalarGrid) -> None:  # noqa: A002
         s = self.sim

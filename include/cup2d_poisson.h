@@ -84,6 +84,14 @@ typedef struct cup2d_solve_opts {
                               refinement of restarted FP32 BiCGSTAB sweeps whose
                               solution update is accumulated in FP64; 0 keeps the
                               recurrences running (reliable updates) */
+  int32_t mean_constraint; /* sim.bMeanConstraint (0 by default): nonzero replaces the
+                              equation of cell (0,0) of the leaf at the domain's (0,0)
+                              corner by sum(h^2 x) = 0 with right-hand side 0
+                              (ExpAMRSolver.cpp:251-256, 340-346; BiCGSTAB.cu:393-410).
+                              FP64 single solves and the server only: the mixed
+                              precision (whose FP32 sweeps derail on the constrained
+                              system), a batch and cup2d_poisson_solve_device_noalloc
+                              reject it with CUP2D_INVALID_ARGUMENT. */
 } cup2d_solve_opts;
 
 typedef struct cup2d_solve_stats {

@@ -59,7 +59,6 @@ class PoissonSolver {
 class ExpAMRSolver : public PoissonSolver {
  public:
   ExpAMRSolver(SimulationData& s, const cup2d_forest& forest) : sim_(s) {
-    if (s.bMeanConstraint != 0) throw std::invalid_argument("bMeanConstraint != 0 is not supported");
     cup2d_solve_opts o = opts();
     check(cup2d_poisson_create(&forest, &o, &h_), "cup2d_poisson_create");
     sim_.UpdateFluxCorrection = false;
@@ -90,6 +89,7 @@ class ExpAMRSolver : public PoissonSolver {
     o.max_restarts = early ? 100 : sim_.maxPoissonRestarts;
     o.max_iter = sim_.maxPoissonIterations;
     o.precision = sim_.mixedPrecision ? CUP2D_PREC_MIXED : CUP2D_PREC_FP64;
+    o.mean_constraint = sim_.bMeanConstraint;
     return o;
   }
   SimulationData& sim_;

@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
         L.oracle_bicgstab.argtypes = [C.c_void_p, pf, pf, pf, C.c_double, C.c_double, C.c_int, C.c_int,
                                       C.POINTER(OracleStats)]
         L.oracle_subtract_mean.argtypes = [C.c_int64, pf, pf]
+        L.oracle_bicgstab_mean.restype = C.c_int
+        L.oracle_bicgstab_mean.argtypes = [C.c_void_p, pf, pf, pf, C.c_double, C.c_double, C.c_int, C.c_int,
+                                           C.c_int64, pf, C.POINTER(OracleStats)]
         L.oracle_pressure_rhs.restype = C.c_int
         L.oracle_pressure_rhs.argtypes = [C.POINTER(OracleForest), C.c_double, pf, pf, pf, pf, pf, pf]
         L.oracle_pressure_correction.restype = C.c_int
@@ -176,14 +179,20 @@ class Matrix:
 
     def bicgstab(self, b: np.ndarray, x0: np.ndarray | None = None, tol_abs: float = 0.0,
                  tol_rel: float = 1e-8, max_restarts: int = 100, max_iter: int = 1000,
-                 P: np.ndarray | None = None):
-        """BiCGSTABSolver::main; returns (x_opt, stats dict)."""
+                 P: np.ndarray | None = None, mean_row: int = -1, h_block: np.ndarray | None = None):
+        """BiCGSTABSolver::main; returns (x_opt, stats dict).  mean_row >= 0:
+        the bMeanConstraint SpMV (that row is sum h^2 x, h_block per block)."""
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
         P = pinv() if P is None else np.ascontiguousarray(P, dtype=np.float64)
         st = OracleStats()
-        lib().oracle_bicgstab(self._h, _pd(P), _pd(b), _pd(x), tol_abs, tol_rel, max_restarts, max_iter,
-                              C.byref(st))
+        if mean_row >= 0:
+            h = np.ascontiguousarray(h_block, dtype=np.float64)
+            lib().oracle_bicgstab_mean(self._h, _pd(P), _pd(b), _pd(x), tol_abs, tol_rel, max_restarts, max_iter,
+                                       int(mean_row), _pd(h), C.byref(st))
+        else:
+            lib().oracle_bicgstab(self._h, _pd(P), _pd(b), _pd(x), tol_abs, tol_rel, max_restarts, max_iter,
+                                  C.byref(st))
         return x, st.as_dict()
 
 
@@ -202,11 +211,28 @@ def subtract_mean(h_block: np.ndarray, x: np.ndarray) -> np.ndarray:
     return x
 
 
+def mean_row(mesh) -> int:
+    """bMeanConstraint's row: cell (0,0) of the leaf whose index is (0,0)
+    (ExpAMRSolver.cpp:251-256)."""
+    blk = np.flatnonzero((np.asarray(mesh.bx) == 0) & (np.asarray(mesh.by) == 0))
+    if blk.size != 1:
+        raise ValueError("oracle: no single leaf at the domain's corner")
+    return int(blk[0]) * 64
+
+
 def solve(mesh, b: np.ndarray, x0=None, tol_abs=0.0, tol_rel=1e-8, max_restarts=100, max_iter=1000,
-          subtract_mean_=True):
-    """ExpAMRSolver::solve end to end on the CPU: assemble, BiCGSTAB, mean removal."""
+          subtract_mean_=True, mean_constraint=False):
+    """ExpAMRSolver::solve end to end on the CPU: assemble, BiCGSTAB, mean removal.
+    mean_constraint: getVec writes 0 into the mean row of b and the solver
+    runs the bMeanConstraint SpMV."""
     A = Matrix(mesh)
-    x, st = A.bicgstab(b, x0, tol_abs, tol_rel, max_restarts, max_iter)
+    if mean_constraint:
+        row = mean_row(mesh)
+        b = np.array(b, dtype=np.float64, copy=True)
+        b[row] = 0.0
+        x, st = A.bicgstab(b, x0, tol_abs, tol_rel, max_restarts, max_iter, mean_row=row, h_block=mesh.cell_h())
+    else:
+        x, st = A.bicgstab(b, x0, tol_abs, tol_rel, max_restarts, max_iter)
     if subtract_mean_:
         x = subtract_mean(mesh.cell_h(), x)
     return x, st

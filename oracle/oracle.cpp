@@ -16,7 +16,9 @@
 //   * Solver: BiCGSTABSolver::main, source/Poisson/BiCGSTAB.cu:412-620 —
 //     right-preconditioned BiCGSTAB, eps = 1e-21, restart on
 //     rho^2 < 1e-16 |r|^2 |rhat|^2, best iterate x_opt by L-inf residual,
-//     stop at |r|_inf <= abs or |r|_inf/|r0|_inf <= rel, 1000-iteration cap.
+//     stop at |r|_inf <= abs or |r|_inf/|r0|_inf <= rel, 1000-iteration cap;
+//     with bMeanConstraint, the SpMV's mean row replaced by sum h^2 x
+//     (BiCGSTAB.cu:393-410).
 //   * Mean removal: ExpAMRSolver::solve, ExpAMRSolver.cpp:383-415.
 //
 // Cubism (the AMR grid library of CUP2D) is an un-vendored submodule, so its
@@ -420,10 +422,26 @@ void precond(int64_t nb, const double* P, const double* p, double* z) {
     }
 }
 
-// BiCGSTABSolver::main, BiCGSTAB.cu:412-620 (single rank, bMeanConstraint=0)
+// bMeanConstraint (BiCGSTAB.cu:393-410): after the SpMV, row mean_row of the
+// result holds sum_i h_i^2 op_i over the operand (blockDscal then a sum).
+struct MeanRow {
+  int64_t row = -1;
+  const double* h_block = nullptr;
+};
+
+void spmv_mean(const Csr& A, const MeanRow& mr, const double* x, double* y) {
+  spmv(A, x, y);
+  if (mr.row < 0) return;
+  double s = 0.0;
+  for (int64_t i = 0; i < A.n; ++i) s += (mr.h_block[i / BLEN] * mr.h_block[i / BLEN]) * x[i];
+  y[mr.row] = s;
+}
+
+// BiCGSTABSolver::main, BiCGSTAB.cu:412-620 (single rank); with mr.row >= 0
+// the bMeanConstraint SpMV (b already holds 0 in that row, as getVec leaves it)
 void bicgstab(const Csr& A, const double* P, const double* b, double* x,
               double max_error, double max_rel_error, int max_restarts,
-              int max_iter, oracle_stats* st) {
+              int max_iter, oracle_stats* st, const MeanRow& mr = MeanRow{}) {
   const int64_t m = A.n, nb = m / BLEN;
   std::vector<double> r(b, b + m), rhat(m), p(m, 0.0), nu(m, 0.0), t(m), z(m), xopt(m);
   double alpha = 1., beta = 1., omega = 1., eps = 1e-21, rho_prev = 1., rho_curr = 1.;
@@ -432,7 +450,7 @@ void bicgstab(const Csr& A, const double* P, const double* b, double* x,
   bool bConverged = false;
   int restarts = 0;
 
-  spmv(A, x, nu.data());                                   // nu = A x0
+  spmv_mean(A, mr, x, nu.data());                          // nu = A x0
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < m; ++i) r[i] = b[i] - nu[i];     // r = b - A x0
   const double nax0 = amax(m, nu.data());
@@ -468,7 +486,7 @@ void bicgstab(const Csr& A, const double* P, const double* b, double* x,
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < m; ++i) p[i] = r[i] + beta * (p[i] - omega * nu[i]);
     precond(nb, P, p.data(), z.data());
-    spmv(A, z.data(), nu.data());
+    spmv_mean(A, mr, z.data(), nu.data());
     const double rn = dot(m, rhat.data(), nu.data());
     alpha = rho_curr / (rn + eps);
 #pragma omp parallel for schedule(static)
@@ -477,7 +495,7 @@ void bicgstab(const Csr& A, const double* P, const double* b, double* x,
       r[i] -= alpha * nu[i];  // s
     }
     precond(nb, P, r.data(), z.data());
-    spmv(A, z.data(), t.data());
+    spmv_mean(A, mr, z.data(), t.data());
     const double ts = dot(m, t.data(), r.data());
     const double tt = dot(m, t.data(), t.data());
     omega = ts / (tt + eps);
@@ -574,6 +592,17 @@ int oracle_bicgstab(const oracle_matrix* M, const double* P, const double* b, do
                     double max_error, double max_rel_error, int max_restarts,
                     int max_iter, oracle_stats* st) {
   bicgstab(M->A, P, b, x, max_error, max_rel_error, max_restarts, max_iter, st);
+  return 0;
+}
+
+// The same with bMeanConstraint: row mean_row is sum(h^2 x) (h per block).
+int oracle_bicgstab_mean(const oracle_matrix* M, const double* P, const double* b, double* x,
+                         double max_error, double max_rel_error, int max_restarts, int max_iter,
+                         int64_t mean_row, const double* h_block, oracle_stats* st) {
+  MeanRow mr;
+  mr.row = mean_row;
+  mr.h_block = h_block;
+  bicgstab(M->A, P, b, x, max_error, max_rel_error, max_restarts, max_iter, st, mr);
   return 0;
 }
 

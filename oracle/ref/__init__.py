@@ -58,6 +58,10 @@ def _load(kind: str) -> C.CDLL:
     L.ref_solve.restype = C.c_int
     L.ref_solve.argtypes = [C.POINTER(RefForest), pd, pd, C.c_double, C.c_double, C.c_int, C.c_int,
                             C.c_char_p, C.c_int64]
+    L.ref_solve_mc.restype = C.c_int
+    L.ref_solve_mc.argtypes = [C.POINTER(RefForest), pd, pd, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                               C.c_char_p, C.c_int64]
+    L.ref_mean_row.restype = C.c_int
     L.ref_copy_pinv.restype = C.c_int
     L.ref_copy_pinv.argtypes = [pd]
     L.ref_system_size.restype = C.c_int
@@ -79,23 +83,26 @@ def _pd(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def _run(L, mesh, b, x, tol_abs, tol_rel, max_restarts, step):
+def _run(L, mesh, b, x, tol_abs, tol_rel, max_restarts, step, mean_constraint=0):
     f, keep = _forest(mesh)
     buf = C.create_string_buffer(1 << 20)
-    rc = L.ref_solve(C.byref(f), _pd(b), _pd(x), tol_abs, tol_rel, max_restarts, step, buf, len(buf))
+    rc = L.ref_solve_mc(C.byref(f), _pd(b), _pd(x), tol_abs, tol_rel, max_restarts, step, int(mean_constraint), buf,
+                        len(buf))
     log = buf.value.decode(errors="replace")
     if rc != 0:
         raise RuntimeError("reference checker failed: " + log.strip().splitlines()[-1] if log.strip() else "")
     return log
 
 
-def assemble(mesh, b: np.ndarray | None = None) -> dict:
-    """The reference's P^-1 and assembled system for the mesh (CPU build)."""
+def assemble(mesh, b: np.ndarray | None = None, mean_constraint: int = 0) -> dict:
+    """The reference's P^-1 and assembled system for the mesh (CPU build);
+    with mean_constraint also the row getMat picks ("mean_row")."""
     L = _load("cpu")
     n = mesh.nblocks * 64
     b = np.zeros(n) if b is None else np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros(n)
-    _run(L, mesh, b, x, 0.0, 0.0, 100, 10)
+    _run(L, mesh, b, x, 0.0, 0.0, 100, 10, mean_constraint)
+    mean_row = int(L.ref_mean_row())
     P = np.empty(64 * 64)
     if L.ref_copy_pinv(_pd(P)) != 0:
         raise RuntimeError("reference checker recorded no P^-1")
@@ -108,7 +115,8 @@ def assemble(mesh, b: np.ndarray | None = None) -> dict:
     bb, x0, h2 = np.empty(m.value), np.empty(m.value), np.empty(m.value // 64)
     L.ref_copy_system(row.ctypes.data_as(C.POINTER(C.c_int32)), col.ctypes.data_as(C.POINTER(C.c_int32)),
                       _pd(val), _pd(bb), _pd(x0), _pd(h2))
-    return {"pinv": P.reshape(64, 64), "row": row, "col": col, "val": val, "b": bb, "x0": x0, "h2": h2}
+    return {"pinv": P.reshape(64, 64), "row": row, "col": col, "val": val, "b": bb, "x0": x0, "h2": h2,
+            "mean_row": mean_row}
 
 
 _NUM = r"([-+0-9.eE]+|inf|nan)"
@@ -140,13 +148,14 @@ def parse_log(log: str) -> dict:
 
 
 def solve(mesh, b: np.ndarray, x0: np.ndarray | None = None, tol_abs: float = 0.0, tol_rel: float = 1e-8,
-          max_restarts: int = 100) -> tuple[np.ndarray, dict]:
+          max_restarts: int = 100, mean_constraint: int = 0) -> tuple[np.ndarray, dict]:
     """ExpAMRSolver::solve with the reference's GPU BiCGSTAB (GPU build).  The
-    call runs with sim.step = 10, where the caller's tolerances apply."""
+    call runs with sim.step = 10, where the caller's tolerances apply, and
+    sim.bMeanConstraint = mean_constraint."""
     L = _load("gpu")
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros(mesh.nblocks * 64) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
-    log = _run(L, mesh, b, x, tol_abs, tol_rel, max_restarts, 10)
+    log = _run(L, mesh, b, x, tol_abs, tol_rel, max_restarts, 10, mean_constraint)
     st = parse_log(log)
     st["log"] = log
     return x, st

@@ -18,7 +18,7 @@
 //
 // The SimulationData members this path reads are set from the arguments:
 // step (tolerances apply from step 10 on, ExpAMRSolver.cpp:366-368),
-// PoissonTol, PoissonTolRel, maxPoissonRestarts, bMeanConstraint = 0.
+// PoissonTol, PoissonTolRel, maxPoissonRestarts, bMeanConstraint.
 #include <cstdint>
 #include <cstring>
 #include <iostream>
@@ -61,8 +61,9 @@ typedef struct ref_forest {
 // reference's mean-removed solution (GPU build) or is unchanged apart from the
 // mean removal (CPU build).  Vectors are block-major, 64 cells per block in
 // iy*8+ix order.  Returns 0, or -1 with the exception text in the log.
-int ref_solve(const ref_forest* f, const double* b, double* x, double tol_abs, double tol_rel, int max_restarts,
-              int step, char* log, int64_t log_cap) {
+// With mean_constraint != 0 the solve runs with sim.bMeanConstraint set.
+int ref_solve_mc(const ref_forest* f, const double* b, double* x, double tol_abs, double tol_rel, int max_restarts,
+                 int step, int mean_constraint, char* log, int64_t log_cap) {
   std::ostringstream out;
   std::streambuf* saved = std::cout.rdbuf(out.rdbuf());
   int rc = 0;
@@ -95,7 +96,7 @@ int ref_solve(const ref_forest* f, const double* b, double* x, double tol_abs, d
       sim.PoissonTol = tol_abs;
       sim.PoissonTolRel = tol_rel;
       sim.maxPoissonRestarts = max_restarts;
-      sim.bMeanConstraint = 0;
+      sim.bMeanConstraint = mean_constraint;
       sim.verbose = false;
       sim.tmp = tmp.get();
       sim.pres = pres.get();
@@ -124,6 +125,15 @@ int ref_solve(const ref_forest* f, const double* b, double* x, double tol_abs, d
   }
   return rc;
 }
+
+int ref_solve(const ref_forest* f, const double* b, double* x, double tol_abs, double tol_rel, int max_restarts,
+              int step, char* log, int64_t log_cap) {
+  return ref_solve_mc(f, b, x, tol_abs, tol_rel, max_restarts, step, 0, log, log_cap);
+}
+
+// The row getMat recorded for bMeanConstraint in the last ref_solve (CPU
+// build; -1 when the constraint was off).
+int ref_mean_row(void) { return ref_capture().have_system ? ref_capture().mean_row : -2; }
 
 // P^-1 recorded by the last ref_solve (CPU build): 64x64, row-major.
 int ref_copy_pinv(double* P) {

@@ -7,6 +7,10 @@ checker built from CUP2D's own Poisson sources (oracle/ref, oracle/_ref).
       values, in the order LocalSpMatDnVec holds them) and of its P^-1, with
       sizes.  -> ref_assembly.json
 
+  python tests/golden/make_ref_fixtures.py mean [--out DIR]
+      GPU.  The same for the bMeanConstraint cases of MEAN_CASES (solved with
+      sim.bMeanConstraint = 1).  -> ref_solve_<case>.npz
+
   python tests/golden/make_ref_fixtures.py solve [--out DIR]
       GPU.  For every case in SOLVE_CASES: ExpAMRSolver::solve with the
       reference's cuBLAS/cuSPARSE BiCGSTAB (x0 = 0, the case's tolerances),
@@ -51,7 +55,13 @@ def assembly_meshes() -> dict:
 
 
 def mesh_by_name(name: str):
-    """Rebuilds a fixture's mesh from its name (the tests use this)."""
+    """Rebuilds a fixture's mesh from its name (the tests use this); a
+    "_rev" suffix lists the named mesh's blocks in reverse order."""
+    if name.endswith("_rev"):
+        from cup2d_b200.mesh import Mesh
+        m = mesh_by_name(name[:-4])
+        return Mesh(m.bpdx, m.bpdy, m.level_max, m.extent, m.level[::-1], m.bx[::-1], m.by[::-1], m.periodic_x,
+                    m.periodic_y)
     if name.startswith("batch_"):
         from cup2d_b200.problems import batch_problems
         return batch_problems(512, seed=3)[int(name.split("_")[1])]
@@ -87,6 +97,23 @@ SOLVE_CASES = {
     "batch_320_1e8": ("batch_320", 100, 0.0, 1e-8),
     "batch_156_1e8": ("batch_156", 101, 0.0, 1e-8),
 }
+
+
+# bMeanConstraint cases: case -> (mesh name, rhs seed, tol_abs, tol_rel, constant
+# added to the right-hand side).  A constant makes the Neumann problem
+# incompatible; the constrained system is regular and solves it anyway.
+MEAN_CASES = {
+    "mean_small": ("small", 1, 0.0, 1e-8, 0.0),
+    "mean_small_shift": ("small", 1, 0.0, 1e-8, 0.25),
+    "mean_periodic_xy_rev": ("periodic_xy_rev", 3, 0.0, 1e-8, -0.1),
+    "mean_sized_1500_rev": ("sized_1500_rev", 2, 0.0, 1e-8, 0.05),
+}
+
+
+def mean_case_rhs(case: str):
+    mesh_name, seed, _, _, shift = MEAN_CASES[case]
+    m = mesh_by_name(mesh_name)
+    return m, m.rhs_fourier(seed) + shift
 
 
 def coo_digest(row: np.ndarray, col: np.ndarray, val: np.ndarray) -> str:
@@ -148,9 +175,33 @@ def make_solve(out: Path, cases: list[str]) -> None:
               flush=True)
 
 
+def make_mean(out: Path, cases: list[str]) -> None:
+    import oracle.ref as R
+    for case in cases:
+        mesh_name, seed, tol_abs, tol_rel, shift = MEAN_CASES[case]
+        m, b = mean_case_rhs(case)
+        t = time.time()
+        x, st = R.solve(m, b, tol_abs=tol_abs, tol_rel=tol_rel, mean_constraint=1)
+        dt = time.time() - t
+        s = sample_stride(m.ncells)
+        h2 = np.repeat(m.cell_h() ** 2, 64)
+        np.savez_compressed(
+            out / f"ref_solve_{case}.npz", x_sample=x[::s], stride=np.int64(s), ncells=np.int64(m.ncells),
+            x_norm2=np.float64(np.linalg.norm(x)), x_absmax=np.float64(np.abs(x).max()),
+            x_h2_sum=np.float64(np.dot(h2, x)), rhs_sha256=np.array(array_digest(b)),
+            mesh=np.array(mesh_name), seed=np.int64(seed), shift=np.float64(shift), mean_constraint=np.int64(1),
+            tol_abs=np.float64(tol_abs), tol_rel=np.float64(tol_rel), iterations=np.int64(st["iterations"] or -1),
+            converged=np.bool_(st["converged"]), restarts=np.int64(st["restarts"]),
+            err_init=np.float64(st["err_init"]), err_opt=np.float64(st["err_opt"]),
+            norm_ax0=np.float64(st["norm_ax0"]), log=np.array(st["log"]))
+        print(f"{case}: {m.nblocks} blocks, iterations {st['iterations']}, converged {st['converged']}, "
+              f"restarts {st['restarts']}, err {st['err_init']:.3e} -> {st['err_opt']:.3e}, {dt:.1f} s",
+              flush=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["assembly", "solve"])
+    ap.add_argument("what", choices=["assembly", "solve", "mean"])
     ap.add_argument("--out", default=str(HERE))
     ap.add_argument("--cases", default=",".join(SOLVE_CASES))
     a = ap.parse_args()
@@ -158,6 +209,8 @@ def main() -> int:
     out.mkdir(parents=True, exist_ok=True)
     if a.what == "assembly":
         make_assembly(out)
+    elif a.what == "mean":
+        make_mean(out, list(MEAN_CASES) if a.cases == ",".join(SOLVE_CASES) else a.cases.split(","))
     else:
         make_solve(out, a.cases.split(","))
     return 0
