@@ -31,6 +31,13 @@ import sys
 import time
 from pathlib import Path
 
+# Hardware work queues per context.  CUDA's default of 8 maps the serving
+# workload's 24 solve streams and 8 assembly streams onto 8 queues, where an
+# assembly kernel can wait behind an unrelated persistent solve that shares
+# its queue; 32 (the maximum) gives every stream its own.  Read when the
+# CUDA context is created, so it is set before anything touches CUDA.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 

@@ -175,6 +175,10 @@ __global__ void k_classify(ForestDev F, int32_t* __restrict__ nbr, unsigned long
   const int64_t i = F.bx[b], j = F.by[b];
   if (l < 0 || l >= F.L || i < 0 || j < 0 || i >= F.nx(l) || j >= F.ny(l)) {
     atomicExch(err, 1);  // reported by k_fill_tables too; never index with it
+    for (int f = 0; f < 4; ++f) nbr[4 * b + f] = kWall;
+    xmask[b] = 0ull;     // no explicit rows: the row pass skips the block
+    xcount[b] = 0;
+    hblk[b] = 0.0;
     return;
   }
   // a leaf must not have a leaf ancestor
@@ -487,12 +491,16 @@ __global__ void __launch_bounds__(64) k_rows(ForestDev Fd, const unsigned long l
                                              const int32_t* __restrict__ xbase, int32_t* __restrict__ rowlen,
                                              int32_t* __restrict__ rowcell, const int32_t* __restrict__ xptr,
                                              int32_t* __restrict__ xcol, double* __restrict__ xval, int pass,
-                                             int* __restrict__ err) {
+                                             int64_t cap, int* __restrict__ err) {
   const int64_t b = blockIdx.x;
   const int c = threadIdx.x;
-  const unsigned long long m = xmask[b];
+  const unsigned long long m = xmask[b];  // 0 for a block k_classify rejected
   if (!((m >> c) & 1ull)) return;
-  const int r = xbase[b] + __popcll(m & ((1ull << c) - 1ull));
+  const int64_t r = xbase[b] + __popcll(m & ((1ull << c) - 1ull));
+  if (r < 0 || r >= cap) {  // never for masks k_classify wrote; keep every index valid
+    atomicExch(err, 6);
+    return;
+  }
   RowAcc row;
   build_row(Fd, b, c & 7, c >> 3, row, err);
   if (pass == 0) {
@@ -537,45 +545,41 @@ int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s) {
   k_classify<<<g, 256, 0, s>>>(F, out.nbr, out.xmask, out.xcount, out.hblk, in.h0, out.err);
   k_origin<<<1, 1, 0, s>>>(F, out.err + 1);
   launch_exclusive_scan(out.xcount, nb, out.xbase, out.scan_tmp, s);
+  // Row arrays at their bound (a block's explicit rows are cells of its four
+  // faces: at most 28), so that the row lengths are built and scanned before
+  // the host knows the row count: one host round trip reads the row count,
+  // the non-zero count and the error flags together.
+  const int64_t cap = kMaxExplicitRowsPerBlock * nb;
+  int st = out.alloc_rows(out.ctx, cap);
+  if (st != CUP2D_OK) return st;
+  if (cudaMemsetAsync(out.rowlen, 0, sizeof(int32_t) * cap, s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.rowcell, nullptr, nullptr, nullptr, 0,
+                                     cap, out.err);
+  launch_exclusive_scan(out.rowlen, cap, out.xptr, out.scan_tmp, s);
   if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
-  int32_t hR = 0;
+  int32_t hR = 0, hnnz = 0;
   int herr[2] = {0, -1};
   if (cudaMemcpyAsync(&hR, out.xbase + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&hnnz, out.xptr + cap, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaMemcpyAsync(herr, out.err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return CUP2D_CUDA_ERROR;
-  if (herr[0] != 0 || herr[1] < 0) return CUP2D_BAD_MESH;
+  if (herr[0] != 0 || herr[1] < 0 || hR > cap) return CUP2D_BAD_MESH;
   out.origin = herr[1];
   out.R = hR;
-  int st = out.alloc_rows(out.ctx, hR);
-  if (st != CUP2D_OK) return st;
-  if (hR > 0) {
-    k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.rowcell, nullptr, nullptr, nullptr,
-                                       0, out.err);
-    launch_exclusive_scan(out.rowlen, hR, out.xptr, out.scan_tmp, s);
-  } else {
-    cudaMemsetAsync(out.xptr, 0, sizeof(int32_t), s);
-  }
-  if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
-  int32_t hnnz = 0;
-  if (cudaMemcpyAsync(&hnnz, out.xptr + hR, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  if (herr[0] != 0) return CUP2D_BAD_MESH;
   out.nnz = hnnz;
   st = out.alloc_nnz(out.ctx, hnnz);
   if (st != CUP2D_OK) return st;
   if (hR > 0) {
+    // the same rows as the length pass (build_row is deterministic): any
+    // malformed face was flagged there already
     k_rows<<<(unsigned)nb, 64, 0, s>>>(F, out.xmask, out.xbase, out.rowlen, out.rowcell, out.xptr, out.xcol,
-                                       out.xval, 1, out.err);
+                                       out.xval, 1, cap, out.err);
     launch_convert_f64_f32(out.xval, out.xval32, hnnz, s);
   }
-  if (cudaGetLastError() != cudaSuccess) return CUP2D_CUDA_ERROR;
-  if (cudaMemcpyAsync(herr, out.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return CUP2D_CUDA_ERROR;
-  return herr[0] != 0 ? CUP2D_BAD_MESH : CUP2D_OK;
+  // the operator is complete when this returns: solves on other streams use it
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
 }
 
 int64_t leaf_table_entries(int bpdx, int bpdy, int level_max) {

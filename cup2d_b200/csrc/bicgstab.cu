@@ -45,6 +45,8 @@
 // only on the true FP64 residual.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <type_traits>
 
@@ -1120,7 +1122,9 @@ cudaError_t allow_smem(const void* fn) {
   return e;
 }
 
-int coop_grid(const void* fn, int device) {
+// The largest co-resident grid of a solve kernel on a device: queried once
+// per device and kernel (handles are created often, e.g. by a server).
+int coop_grid_query(const void* fn, int device) {
   int sms = 0, per_sm = 0, cur = 0;
   if (cudaGetDevice(&cur) != cudaSuccess) return 0;
   if (cur != device && cudaSetDevice(device) != cudaSuccess) return 0;
@@ -1130,6 +1134,18 @@ int coop_grid(const void* fn, int device) {
                       cudaSuccess;
   if (cur != device) cudaSetDevice(cur);
   return ok ? sms * per_sm : 0;
+}
+
+int coop_grid(const void* fn, int device) {
+  static std::atomic<int> cache[64][kNumSolveFns];
+  int k = 0;
+  while (k < kNumSolveFns && kSolveFns[k] != fn) ++k;
+  if (device < 0 || device >= 64 || k == kNumSolveFns) return coop_grid_query(fn, device);
+  int g = cache[device][k].load(std::memory_order_acquire);
+  if (g > 0) return g;
+  g = coop_grid_query(fn, device);
+  if (g > 0) cache[device][k].store(g, std::memory_order_release);
+  return g;
 }
 }  // namespace
 

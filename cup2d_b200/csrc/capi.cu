@@ -306,6 +306,15 @@ int do_assemble(cup2d_poisson* h, const cup2d_forest* f) {
   return assemble_blocks(h, f, nb);
 }
 
+// The timing events of a handle (made on first use for handles that were
+// created on a caller's stream).
+int ensure_events(cup2d_poisson* h) {
+  if (h->ev0 && h->ev1) return CUP2D_OK;
+  if ((!h->ev0 && cudaEventCreate(&h->ev0) != cudaSuccess) || (!h->ev1 && cudaEventCreate(&h->ev1) != cudaSuccess))
+    return CUP2D_CUDA_ERROR;
+  return CUP2D_OK;
+}
+
 int ensure_scratch(cup2d_poisson* h) {
   int st;
   const int g = std::max(h->grid64, h->gridmx);
@@ -394,6 +403,15 @@ int cup2d_pinv(double* P_out) {
 }
 
 int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cup2d_poisson** out) {
+  return handle_create(forest, opts, nullptr, out);
+}
+
+}  // extern "C"
+
+namespace cup2d {
+
+int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cudaStream_t stream,
+                  cup2d_poisson** out) {
   if (!out) return CUP2D_INVALID_ARGUMENT;
   *out = nullptr;
   cup2d_solve_opts o;
@@ -415,12 +433,17 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
   // priority: when a server assembles a new mesh while persistent solves
   // hold most of the device, its short assembly kernels take the CTA slots
   // that free up before queued solve work does
-  int prio_lo = 0, prio_hi = 0;
-  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
-  if (cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
-    cup2d_poisson_destroy(h);
-    return CUP2D_CUDA_ERROR;
+  if (stream) {  // the caller's (a server's assembly stream): no stream or events of its own
+    h->stream = stream;
+    h->owns_stream = false;
+  } else {
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        ensure_events(h) != CUP2D_OK) {
+      cup2d_poisson_destroy(h);
+      return CUP2D_CUDA_ERROR;
+    }
   }
   h->grid64 = max_coop_grid_fp64(h->device);
   h->gridmx = max_coop_grid_mixed(h->device);
@@ -443,6 +466,10 @@ int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opt
   *out = h;
   return CUP2D_OK;
 }
+
+}  // namespace cup2d
+
+extern "C" {
 
 int cup2d_poisson_update_mesh(cup2d_poisson* h, const cup2d_forest* forest) {
   if (!h) return CUP2D_INVALID_ARGUMENT;
@@ -609,6 +636,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     h->hstats = nullptr;
     return CUP2D_OOM;
   }
+  if (stats && (st = ensure_events(h))) return st;
   if (stats) cudaEventRecord(h->ev0, s);
   cudaError_t e;
   if (o.precision == CUP2D_PREC_MIXED) {

@@ -64,6 +64,9 @@ struct DeviceMesh {
   }
 };
 
+// Explicit (coarse/fine) rows of one block at most: the cells on its four faces.
+constexpr int64_t kMaxExplicitRowsPerBlock = 28;
+
 int64_t leaf_table_entries(int bpdx, int bpdy, int level_max);
 int64_t scan_temp_ints(int64_t n);
 int assemble_on_device(const AssembleIn& in, DeviceMesh& out, cudaStream_t s);

@@ -122,16 +122,21 @@ struct cup2d_server {
   std::condition_variable asm_cv;   // meshes to assemble
   std::thread worker;
   std::vector<std::thread> assemblers;
+  // one assembly stream per assembler thread, at the highest priority, made
+  // once: a handle created per request would otherwise make (and destroy)
+  // a stream and two events every time, which under load took as long as
+  // the assembly itself; the handles of a thread assemble on its stream
+  std::vector<cudaStream_t> asm_streams;
   std::deque<int64_t> completed_q;  // finished requests not yet taken
   static constexpr int kAssemblers = 8;
   bool stop = false;
   int fatal = CUP2D_OK;  // a CUDA error that stopped the worker
 
   void run();
-  void run_assembler();
+  void run_assembler(cudaStream_t stream);
   bool complete_slots();  // mu held
   bool admit();           // mu held
-  int assemble(Mesh& m, std::unique_lock<std::mutex>& lk);
+  int assemble(Mesh& m, std::unique_lock<std::mutex>& lk, cudaStream_t stream);
   int launch(Slot& s, int64_t rid, Request& r, Mesh& m);
   // CTAs of a mesh's solves: opts.team, or by size when it is 0
   int team_for(int64_t nb) const {
@@ -156,7 +161,7 @@ int server_error(cup2d_server* S, int st) {
 // Makes m resident: evicts idle meshes (least recently used first) until it
 // fits the budget, then assembles it with the lock released.  Returns
 // CUP2D_QUEUE_FULL when the memory is held by meshes in use.
-int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
+int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk, cudaStream_t stream) {
   const int64_t need = m.estimate_bytes();
   if (need > budget) return CUP2D_OOM;
   while (resident_bytes + need > budget) {
@@ -180,7 +185,7 @@ int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
   resident_bytes += need;  // reserved while assembling
   lk.unlock();
   const Clock::time_point t_asm = Clock::now();
-  int st = cup2d_poisson_create(&f, &o, &h);
+  int st = handle_create(&f, &o, stream, &h);
   if (st == CUP2D_OK) st = cup2d_poisson_set_grid(h, team);
   double* db = nullptr;
   double* dx = nullptr;
@@ -202,7 +207,7 @@ int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk) {
   return CUP2D_OK;
 }
 
-void cup2d_server::run_assembler() {
+void cup2d_server::run_assembler(cudaStream_t stream) {
   cudaSetDevice(device);
   std::unique_lock<std::mutex> lk(mu);
   while (!stop) {
@@ -213,7 +218,7 @@ void cup2d_server::run_assembler() {
     const int64_t id = to_assemble.front();
     to_assemble.pop_front();
     Mesh& m = meshes.at(id);
-    const int st = assemble(m, lk);
+    const int st = assemble(m, lk, stream);
     if (st == CUP2D_QUEUE_FULL) {
       // the budget is held by meshes in use: retry after a completion
       to_assemble.push_back(id);
@@ -419,6 +424,8 @@ int cup2d_server_destroy(cup2d_server* S) {
   }
   for (auto& kv : S->meshes)
     if (kv.second.h) handle_destroy_idle(kv.second.h);  // every slot stream is synchronised
+  for (cudaStream_t st : S->asm_streams)  // after the handles that assembled on them
+    if (st) cudaStreamDestroy(st);
   delete S;
   return CUP2D_OK;
 }
@@ -466,8 +473,20 @@ int cup2d_server_create(const cup2d_server_opts* opts, cup2d_server** out) {
     return CUP2D_CUDA_ERROR;
   }
   S->cta_cap = std::max(1, (int)(o.solve_share * grid_max));
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  S->asm_streams.assign(cup2d_server::kAssemblers, nullptr);
+  for (cudaStream_t& st : S->asm_streams)
+    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
+      st = nullptr;
+      cup2d_server_destroy(S);
+      return CUP2D_CUDA_ERROR;
+    }
   S->worker = std::thread([S] { S->run(); });
-  for (int i = 0; i < cup2d_server::kAssemblers; ++i) S->assemblers.emplace_back([S] { S->run_assembler(); });
+  for (int i = 0; i < cup2d_server::kAssemblers; ++i) {
+    cudaStream_t st = S->asm_streams[i];
+    S->assemblers.emplace_back([S, st] { S->run_assembler(st); });
+  }
   *out = S;
   return CUP2D_OK;
 }
