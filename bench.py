@@ -161,11 +161,14 @@ def algorithmic_bytes(n: int, nb: int, R: int, nnz: int, iters: int, updates: in
     return setup + iters * per_iter + updates * per_update + final
 
 
-def spmv_leg(dev, stream, steps: int = 20, warmup: int = 5) -> dict:
+def spmv_leg(dev, stream, steps: int = 20, warmup: int = 5, forest: str = "full") -> dict:
     """The operator apply y = A x alone (the library's standalone SpMV, FP64
     and FP32) on one forest far above L2: bpdx=64, bpdy=32, levelMax=6, 3
     seeded disks, band 0.35 (1.15 M blocks, 73 M cells: 1.2 GB of x and y in
-    FP64, so that launch and ramp-up are small against the transfer).
+    FP64, so that launch and ramp-up are small against the transfer).  With
+    forest="small" (profiling captures): bpdx=32, bpdy=16, the same disks and
+    levels, band 0.15 (0.1 M blocks, 6.6 M cells: every kernel's traffic
+    still twice L2 or more).
     Algorithmic bytes per launch:
     read x, write y, the explicit coarse/fine rows (values + column indices +
     row pointers) and 28 B of block structure per block."""
@@ -174,9 +177,10 @@ def spmv_leg(dev, stream, steps: int = 20, warmup: int = 5) -> dict:
 
     from cup2d_b200 import Mesh, Solver
     from cup2d_b200.problems import EXTENT, seeded_disks
-    mesh = Mesh.disks(64, 32, 6, EXTENT, seeded_disks(np.random.default_rng(5), 3), 0.35)
+    bpd, band = ((64, 32), 0.35) if forest == "full" else ((32, 16), 0.15)
+    mesh = Mesh.disks(bpd[0], bpd[1], 6, EXTENT, seeded_disks(np.random.default_rng(5), 3), band)
     n = mesh.ncells
-    out = {"mesh": f"bpdx=64 bpdy=32 levelMax=6, 3 disks, band 0.35: {mesh.nblocks} blocks, {n} cells"}
+    out = {"mesh": f"bpdx={bpd[0]} bpdy={bpd[1]} levelMax=6, 3 disks, band {band}: {mesh.nblocks} blocks, {n} cells"}
     peak, kind = _peaks()
     with Solver(mesh) as h:
         R, nnz = h.explicit_info()
@@ -646,9 +650,50 @@ def run_batch(args, world, rank, local) -> dict | None:
     }
     if not args.no_serve:
         line["serving"] = run_serve_sweep(args)
+    if world == 1 and not args.no_configs:
+        # the other configurations of the benchmark, measured in the same run
+        line["large"] = large_leg(dev, stream)
+        line["timestep"] = run_timestep(args)
     if not args.no_cpu and world == 1:  # the host baseline: rank 0 at N=1 only
         line["cpu_baseline"] = batch_cpu_baseline(meshes, seeds, args.cpu_slices)
     return line
+
+
+def large_leg(dev, stream, solves: int = 2) -> dict:
+    """The large configuration (bpdx=8, bpdy=4, levelMax=7, 3 seeded disks;
+    20,834 blocks) solved from x0 = 0 to true |b-Ax|_inf <= tol |b|_inf, tol
+    1e-6 (the served/batched tolerance) and 1e-8 (the configuration's), plain
+    FP64 and mixed, without the reference's 1000-iteration cap: device time
+    per solve (CUDA events, 256 MiB L2 flush between solves)."""
+    import torch
+
+    from cup2d_b200 import Solver
+    from cup2d_b200.problems import large_mesh
+    mesh = large_mesh()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    bs = [torch.from_numpy(mesh.rhs_fourier(17 + k)).to(dev) for k in range(solves + 1)]
+    x = torch.zeros(mesh.ncells, dtype=torch.float64, device=dev)
+    out = {"mesh": f"{mesh.nblocks} blocks, {mesh.ncells} cells"}
+    with Solver(mesh) as s:
+        for tol in (1e-6, 1e-8):
+            for prec in ("fp64", "mixed"):
+                s.set_opts(tol_rel=tol, max_iter=20000, max_restarts=100, precision=prec)
+                ms, its = [], []
+                for k, b in enumerate(bs):
+                    flush.fill_(float(k))
+                    x.zero_()
+                    # device time of the solve launch: the library's CUDA
+                    # events around it on the launching stream
+                    st = s.solve_device(b, x, stream=stream)
+                    if k == 0:
+                        continue  # warm-up
+                    ms.append(st["solve_ms"])
+                    its.append(st["iterations"])
+                    if st["status"] != 0:
+                        raise RuntimeError(f"large {prec} {tol}: status {st['status']}")
+                out[f"{prec}_{tol:g}"] = {"solves_per_s": 1e3 / statistics.mean(ms), "ms": statistics.mean(ms),
+                                          "iterations_mean": statistics.mean(its)}
+    return out
 
 
 def run_timestep(args) -> dict:
@@ -1024,11 +1069,15 @@ def main(argv=None) -> int:
     ap.add_argument("--no-spmv", action="store_true", help="batch: skip the standalone SpMV leg")
     ap.add_argument("--spmv-only", action="store_true", help="the standalone SpMV leg alone (profiling runs)")
     ap.add_argument("--no-graph", action="store_true", help="batch: launch directly instead of graph replays")
+    ap.add_argument("--spmv-forest", choices=["full", "small"], default="full",
+                    help="with --spmv-only: the forest of the standalone kernel leg (small: for profiling)")
     ap.add_argument("--plain-steps", type=int, default=0,
                     help="batch: timed steps of the one-at-a-time FP64 leg (0 = --steps)")
     ap.add_argument("--cpu-slices", type=int, default=4,
                     help="batch CPU baseline: size-stratified slices (1/64 of the batch each) solved in full")
     ap.add_argument("--no-serve", action="store_true", help="batch: skip the serving leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="batch: skip the large and time-stepping legs that follow the headline")
     ap.add_argument("--serve-rate", type=float, default=100.0, help="serving: offered requests/s (--workload serve)")
     ap.add_argument("--serve-rates", default="100,300,1000",
                     help="batch workload's serving leg: offered rates of the sweep (requests/s)")
@@ -1036,7 +1085,7 @@ def main(argv=None) -> int:
     ap.add_argument("--serve-pool", type=int, default=40, help="serving: distinct forests")
     ap.add_argument("--serve-inflight", type=int, default=24, help="serving: solve slots")
     ap.add_argument("--serve-share", type=float, default=0.9, help="serving: share of solve CTAs in use")
-    ap.add_argument("--serve-bpc", type=int, default=160, help="serving: blocks per CTA of a solve's team")
+    ap.add_argument("--serve-bpc", type=int, default=320, help="serving: blocks per CTA of a solve's team")
     ap.add_argument("--serve-xbufs", type=int, default=12, help="serving: pinned solution buffers per forest")
     ap.add_argument("--headline-only", action="store_true",
                     help="batch: time the batched mixed leg only (for profilers; no comparison legs)")
@@ -1051,7 +1100,8 @@ def main(argv=None) -> int:
         import torch
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
-        print(json.dumps(spmv_leg(dev, torch.cuda.current_stream(dev), steps=args.steps, warmup=args.warmup)))
+        print(json.dumps(spmv_leg(dev, torch.cuda.current_stream(dev), steps=args.steps, warmup=args.warmup,
+                                  forest=args.spmv_forest)))
         return 0
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -395,7 +395,7 @@ void cup2d_server_default_opts(cup2d_server_opts* o) {
   if (!o) return;
   o->max_inflight = 24;
   o->team = 16;
-  o->blocks_per_cta = 160;
+  o->blocks_per_cta = 320;
   o->solve_share = 0.9;
   o->hbm_budget_bytes = 0;
   cup2d_default_opts(&o->solve);

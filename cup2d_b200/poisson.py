@@ -505,7 +505,7 @@ class Server:
     WARM_START = 1
 
     def __init__(self, max_inflight: int = 24, team: int = 16, hbm_budget_bytes: int = 0,
-                 opts: Optional[L.SolveOpts] = None, blocks_per_cta: int = 160, solve_share: float = 0.9,
+                 opts: Optional[L.SolveOpts] = None, blocks_per_cta: int = 320, solve_share: float = 0.9,
                  **kw):
         o = L.ServerOpts()
         L.lib().cup2d_server_default_opts(C.byref(o))

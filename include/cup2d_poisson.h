@@ -363,7 +363,7 @@ typedef struct cup2d_server_opts {
   int32_t max_inflight;      /* solves on the device at once (one stream each); default 24 */
   int32_t team;              /* CTAs per solve; default 16; 0: by mesh size (one CTA per
                                 blocks_per_cta blocks, 2..128) */
-  int32_t blocks_per_cta;    /* with team 0; default 160 */
+  int32_t blocks_per_cta;    /* with team 0; default 320 (measured best of 160/256/320/400/640 at saturation) */
   double solve_share;        /* share of the device's co-resident solve CTAs that solves
                                 may hold at once (the rest stays free for assembly
                                 kernels and copies); default 0.9 */
