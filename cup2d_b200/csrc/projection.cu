@@ -86,8 +86,10 @@ struct Geo {
     if (code != kExplicit) return s;  // domain edge
     const int l = F.level[b];
     const int64_t nx = (int64_t)F.bpdx << l, ny = (int64_t)F.bpdy << l;
-    const int64_t ni = ((int64_t)F.bx[b] + (f == 0 ? -1 : f == 1 ? 1 : 0) + nx) % nx;
-    const int64_t nj = ((int64_t)F.by[b] + (f == 2 ? -1 : f == 3 ? 1 : 0) + ny) % ny;
+    int64_t ni = (int64_t)F.bx[b] + (f == 0 ? -1 : f == 1 ? 1 : 0);
+    int64_t nj = (int64_t)F.by[b] + (f == 2 ? -1 : f == 3 ? 1 : 0);
+    ni = ni < 0 ? ni + nx : ni >= nx ? ni - nx : ni;  // periodic wrap (one step at most)
+    nj = nj < 0 ? nj + ny : nj >= ny ? nj - ny : nj;
     const int32_t c = leaf(l - 1, ni >> 1, nj >> 1);
     if (c >= 0) {
       s.kind = kCoarser;
@@ -144,64 +146,64 @@ __device__ double interp_ghost(const Fld& w, int c, int64_t bc, int xc, int yc, 
   return (kI23 * vclose - kI15 * vfar) + kI815 * tay;
 }
 
-// One cell and its four faces.
-struct CellCtx {
+// The ghost cell of one edge cell of block b across face f: one thread of the
+// block's lab fill (thread g of the block: face g / 8, cell g % 8 along it).
+struct Ghost {
   const Geo& G;
   int64_t b, cell;
-  int ix, iy, l;
-  Side s[4];  // valid for the faces on the block edge
-  __device__ bool on_edge(int f) const {
-    return f == 0 ? ix == 0 : f == 1 ? ix == kBS - 1 : f == 2 ? iy == 0 : iy == kBS - 1;
-  }
-  __device__ int64_t inblock(int f) const {
-    return cidx(b, ix + (f == 0 ? -1 : f == 1 ? 1 : 0), iy + (f == 2 ? -1 : f == 3 ? 1 : 0));
-  }
-  // fine block and the along-face position of the fine cells facing this cell
-  __device__ void fine_cells(int f, int64_t& fb, int& k0) const {
-    const bool xface = f < 2;
-    fb = s[f].fine[xface ? (iy >= kBS / 2) : (ix >= kBS / 2)];
-    k0 = ((xface ? iy : ix) % (kBS / 2)) * 2;
-  }
-  // fine cell q of face f (depth d), as a global cell index
-  __device__ int64_t fine_cell(int f, int64_t fb, int k0, int q, int d) const {
-    return f < 2 ? mirror(f, fb, 0, k0 + q, d) : mirror(f, fb, k0 + q, 0, d);
-  }
+  int ix, iy, f;
+  Side s;
 
-  // Lab value of component c of field w across face f.
-  __device__ double nb(const Fld& w, int c, int f, bool vector) const {
-    if (!on_edge(f)) return w.v(inblock(f), c);
-    const bool xface = f < 2;
-    switch (s[f].kind) {
+  // gi: the ghost's index in the block (face gi / 8); sd: the face's side,
+  // looked up by the caller ahead of its other loads
+  __device__ Ghost(const Geo& g, int64_t blk, int gi, const Side& sd) : G(g), b(blk), f(gi >> 3), s(sd) {
+    const int k = gi & 7;
+    ix = f == 0 ? 0 : f == 1 ? kBS - 1 : k;
+    iy = f == 2 ? 0 : f == 3 ? kBS - 1 : k;
+    cell = cidx(b, ix, iy);
+  }
+  __device__ bool xface() const { return f < 2; }
+  // fine block and the along-face position of the fine cells facing this cell
+  __device__ void fine_cells(int64_t& fb, int& k0) const {
+    fb = s.fine[xface() ? (iy >= kBS / 2) : (ix >= kBS / 2)];
+    k0 = ((xface() ? iy : ix) % (kBS / 2)) * 2;
+  }
+  // fine cell q (depth d), as a global cell index
+  __device__ int64_t fine_cell(int64_t fb, int k0, int q, int d) const {
+    return xface() ? mirror(f, fb, 0, k0 + q, d) : mirror(f, fb, k0 + q, 0, d);
+  }
+  // The lab value of component c of field w in the ghost cell.
+  __device__ double value(const Fld& w, int c, bool vector) const {
+    switch (s.kind) {
       case kSame:
-        return w.v(mirror(f, s[f].blk, ix, iy, 0), c);
+        return w.v(mirror(f, s.blk, ix, iy, 0), c);
       case kEdge: {
         const double own = w.v(cell, c);
-        return (vector && c == (xface ? 0 : 1)) ? -own : own;
+        return (vector && c == (xface() ? 0 : 1)) ? -own : own;
       }
       case kCoarser: {
         const int64_t bx = G.F.bx[b], by = G.F.by[b];
         const int xc = f == 0 ? kBS - 1 : f == 1 ? 0 : (bx % 2 == 0 ? ix / 2 : ix / 2 + kBS / 2);
         const int yc = f == 2 ? kBS - 1 : f == 3 ? 0 : (by % 2 == 0 ? iy / 2 : iy / 2 + kBS / 2);
-        const double sT = xface ? (iy % 2 == 0 ? -1. : 1.) : (ix % 2 == 0 ? -1. : 1.);
+        const double sT = xface() ? (iy % 2 == 0 ? -1. : 1.) : (ix % 2 == 0 ? -1. : 1.);
         const int64_t inward = cidx(b, ix + (f == 0 ? 1 : f == 1 ? -1 : 0), iy + (f == 2 ? 1 : f == 3 ? -1 : 0));
-        return interp_ghost(w, c, s[f].blk, xc, yc, w.v(cell, c), w.v(inward, c), sT, xface);
+        return interp_ghost(w, c, s.blk, xc, yc, w.v(cell, c), w.v(inward, c), sT, xface());
       }
       default: {
         int64_t fb;
         int k0;
-        fine_cells(f, fb, k0);
-        const double s00 = w.v(fine_cell(f, fb, k0, 0, 0), c), s01 = w.v(fine_cell(f, fb, k0, 1, 0), c);
-        const double s10 = w.v(fine_cell(f, fb, k0, 0, 1), c), s11 = w.v(fine_cell(f, fb, k0, 1, 1), c);
+        fine_cells(fb, k0);
+        const double s00 = w.v(fine_cell(fb, k0, 0, 0), c), s01 = w.v(fine_cell(fb, k0, 1, 0), c);
+        const double s10 = w.v(fine_cell(fb, k0, 0, 1), c), s11 = w.v(fine_cell(fb, k0, 1, 1), c);
         return 0.25 * ((s00 + s01) + (s10 + s11));
       }
     }
   }
-
-  // Ghost of fine cell q of finer face f (seen from the fine block), the
+  // Ghost of fine cell q of a finer face (seen from the fine block), the
   // interpolation centred on this coarse cell.
-  __device__ double fine_ghost(const Fld& w, int c, int f, int64_t fb, int k0, int q) const {
-    return interp_ghost(w, c, b, ix, iy, w.v(fine_cell(f, fb, k0, q, 0), c), w.v(fine_cell(f, fb, k0, q, 1), c),
-                        q == 0 ? -1. : 1., f < 2);
+  __device__ double fine_ghost(const Fld& w, int c, int64_t fb, int k0, int q) const {
+    return interp_ghost(w, c, b, ix, iy, w.v(fine_cell(fb, k0, q, 0), c), w.v(fine_cell(fb, k0, q, 1), c),
+                        q == 0 ? -1. : 1., xface());
   }
 };
 
@@ -221,97 +223,185 @@ __device__ __forceinline__ double div_face(int f, double facDiv, double chi, dou
   return s;
 }
 
-__global__ void __launch_bounds__(kProjThreads) k_pressure_rhs(Geo G, double dt, ProjFields P) {
-  const int64_t cell = (int64_t)blockIdx.x * kProjThreads + threadIdx.x;
-  if (cell >= G.F.nb * kBLEN) return;
-  const int64_t b = cell >> 6;
-  const int ci = (int)(cell & 63);
-  CellCtx C{G, b, cell, ci & 7, ci >> 3, G.F.level[b], {}};
-  for (int f = 0; f < 4; ++f)
-    if (C.on_edge(f)) C.s[f] = G.side(b, f);
-  const double h = cell_h(G.F, C.l);
-  double t;
-  if (P.vel) {
-    const Fld V{P.vel, 2}, U{P.udef, 2};
-    const double facDiv = 0.5 * h / dt;
-    const double CHI = P.chi[cell];
-    t = facDiv * ((C.nb(V, 0, 1, true) - C.nb(V, 0, 0, true)) + (C.nb(V, 1, 3, true) - C.nb(V, 1, 2, true)));
-    t += -facDiv * CHI * ((C.nb(U, 0, 1, true) - C.nb(U, 0, 0, true)) + (C.nb(U, 1, 3, true) - C.nb(U, 1, 2, true)));
-    for (int f = 0; f < 4; ++f) {
-      if (!C.on_edge(f) || C.s[f].kind != kFiner) continue;
-      const int c = f < 2 ? 0 : 1;
-      const double own = div_face(f, facDiv, CHI, C.nb(V, c, f, true), V.v(cell, c), C.nb(U, c, f, true), U.v(cell, c));
-      int64_t fb;
-      int k0;
-      C.fine_cells(f, fb, k0);
-      const int lf = G.F.level[fb];
-      const double facDivF = 0.5 * cell_h(G.F, lf) / dt;
-      double fs[2];
-      for (int q = 0; q < 2; ++q) {
-        const int64_t fc = C.fine_cell(f, fb, k0, q, 0);
-        fs[q] = div_face(f ^ 1, facDivF, P.chi[fc], C.fine_ghost(V, c, f, fb, k0, q), V.v(fc, c),
-                         C.fine_ghost(U, c, f, fb, k0, q), U.v(fc, c));
-      }
-      t = t + (own + (fs[0] + fs[1]));
-    }
-  } else {
-    t = P.tmp[cell];
-  }
-  if (P.pres) {
-    const Fld Q{P.pres, 1};
-    const double p0 = Q.v(cell, 0);
-    t -= ((C.nb(Q, 0, 0, false) + C.nb(Q, 0, 1, false)) + (C.nb(Q, 0, 2, false) + C.nb(Q, 0, 3, false))) - 4.0 * p0;
-    for (int f = 0; f < 4; ++f) {
-      if (!C.on_edge(f) || C.s[f].kind != kFiner) continue;
-      const double own = C.nb(Q, 0, f, false) - p0;
-      int64_t fb;
-      int k0;
-      C.fine_cells(f, fb, k0);
-      double fs[2];
-      for (int q = 0; q < 2; ++q) fs[q] = C.fine_ghost(Q, 0, f, fb, k0, q) - Q.v(C.fine_cell(f, fb, k0, q, 0), 0);
-      t = t + (own + (fs[0] + fs[1]));
-    }
-    P.pold[cell] = p0;
-  }
-  P.tmp[cell] = t;
-}
-
 // pressureCorrectionKernel stored face value (PressureSingle.cpp:152-185).
 __device__ __forceinline__ double grad_face(int f, double pFac, double g, double w) {
   return ((f & 1) == 0 ? pFac : -pFac) * (g + w);
 }
 
-__global__ void __launch_bounds__(kProjThreads) k_pressure_correction(Geo G, double dt, const double* __restrict__ pres,
-                                                                     double* __restrict__ vel) {
-  const int64_t cell = (int64_t)blockIdx.x * kProjThreads + threadIdx.x;
-  if (cell >= G.F.nb * kBLEN) return;
-  const int64_t b = cell >> 6;
-  const int ci = (int)(cell & 63);
-  CellCtx C{G, b, cell, ci & 7, ci >> 3, G.F.level[b], {}};
-  for (int f = 0; f < 4; ++f)
-    if (C.on_edge(f)) C.s[f] = G.side(b, f);
-  const Fld Q{pres, 1};
-  const double h = cell_h(G.F, C.l);
-  const double pFac = -0.5 * dt * h;
-  const double p0 = Q.v(cell, 0);
-  double tv[2];
-  tv[0] = pFac * (C.nb(Q, 0, 1, false) - C.nb(Q, 0, 0, false));
-  tv[1] = pFac * (C.nb(Q, 0, 3, false) - C.nb(Q, 0, 2, false));
-  for (int f = 0; f < 4; ++f) {
-    if (!C.on_edge(f) || C.s[f].kind != kFiner) continue;
-    const double own = grad_face(f, pFac, C.nb(Q, 0, f, false), p0);
-    int64_t fb;
-    int k0;
-    C.fine_cells(f, fb, k0);
-    const double pFacF = -0.5 * dt * cell_h(G.F, G.F.level[fb]);
-    double fs[2];
-    for (int q = 0; q < 2; ++q)
-      fs[q] = grad_face(f ^ 1, pFacF, C.fine_ghost(Q, 0, f, fb, k0, q), Q.v(C.fine_cell(f, fb, k0, q, 0), 0));
-    tv[f < 2 ? 0 : 1] = tv[f < 2 ? 0 : 1] + (own + (fs[0] + fs[1]));
+// Labs in shared memory: kLabBlocks blocks per CTA, 64 threads each.  Every
+// thread stages its cell; 32 threads of each block then fill the ghost
+// layer (the face neighbours, the edge rules, the coarse/fine rules) and, on
+// faces with finer neighbours, the flux-correction terms; then every thread
+// evaluates its cell from shared memory.  The stencil threads stay simple,
+// the irregular work is confined to the ghost threads.
+constexpr int kLabBlocks = kProjThreads / kBLEN;
+constexpr int kLab = kBS + 2;
+enum : int { kLabU = 0, kLabV = 1, kLabUd = 2, kLabVd = 3, kLabP = 4, kLabs = 5 };
+
+struct ProjSmem {
+  double lab[kLabs][kLabBlocks][kLab][kLab];
+  double corr[2][kLabBlocks][4][kBS];  // finer faces: [0] divergence / gradient, [1] Laplacian
+  int kind[kLabBlocks][4];
+};
+
+__device__ __forceinline__ double& labv(ProjSmem& S, int q, int lb, int ix, int iy) {
+  return S.lab[q][lb][iy + 1][ix + 1];
+}
+
+__global__ void __launch_bounds__(kProjThreads, 4) k_pressure_rhs(const __grid_constant__ Geo G, double dt,
+                                                                    const __grid_constant__ ProjFields P) {
+  __shared__ ProjSmem S;
+  const int lb = threadIdx.x >> 6, c = threadIdx.x & 63, ix = c & 7, iy = c >> 3;
+  const int64_t b = (int64_t)blockIdx.x * kLabBlocks + lb;
+  const bool valid = b < G.F.nb;
+  const int64_t cell = b * kBLEN + c;
+  const bool vel = P.vel != nullptr, pres = P.pres != nullptr;
+  // ghost work: threads 0-31 of a block the velocity ghosts, 32-63 the
+  // pressure ghosts (ghost index c % 32); the face's side first, so that its
+  // table loads overlap the staging loads
+  const int gi = c & 31;
+  const bool gvel = c < 32 && vel, gpres = c >= 32 && pres;
+  Side sd{kEdge, -1, {-1, -1}};
+  if (valid && (gvel || gpres)) sd = G.side(b, gi >> 3);
+  // stage the block
+  double chi = 0.0, p0 = 0.0;
+  if (valid) {
+    if (vel) {
+      const double2 u = __ldg(reinterpret_cast<const double2*>(P.vel) + cell);
+      const double2 ud = __ldg(reinterpret_cast<const double2*>(P.udef) + cell);
+      chi = __ldg(P.chi + cell);
+      labv(S, kLabU, lb, ix, iy) = u.x;
+      labv(S, kLabV, lb, ix, iy) = u.y;
+      labv(S, kLabUd, lb, ix, iy) = ud.x;
+      labv(S, kLabVd, lb, ix, iy) = ud.y;
+    }
+    if (pres) {
+      p0 = __ldg(P.pres + cell);
+      labv(S, kLabP, lb, ix, iy) = p0;
+    }
   }
+  // ghost layer and flux-correction terms
+  if (valid && (gvel || gpres)) {
+    const Ghost gh(G, b, gi, sd);
+    const int k = gi & 7, f = gh.f;
+    if (k == 0 && c < 32) S.kind[lb][f] = gh.s.kind;
+    const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
+    const double h = cell_h(G.F, G.F.level[b]);
+    if (gvel) {
+      const Fld V{P.vel, 2}, U{P.udef, 2};
+      const int cmp = gh.xface() ? 0 : 1;  // the normal component: the only one the divergence reads
+      const double g = gh.value(V, cmp, true), gd = gh.value(U, cmp, true);
+      labv(S, gh.xface() ? kLabU : kLabV, lb, gx, gy) = g;
+      labv(S, gh.xface() ? kLabUd : kLabVd, lb, gx, gy) = gd;
+      if (gh.s.kind == kFiner) {
+        const double facDiv = 0.5 * h / dt;
+        const double own = div_face(f, facDiv, __ldg(P.chi + gh.cell), g, V.v(gh.cell, cmp), gd, U.v(gh.cell, cmp));
+        int64_t fb;
+        int k0;
+        gh.fine_cells(fb, k0);
+        const double facDivF = 0.5 * cell_h(G.F, G.F.level[fb]) / dt;
+        double fs[2];
+        for (int q = 0; q < 2; ++q) {
+          const int64_t fc = gh.fine_cell(fb, k0, q, 0);
+          fs[q] = div_face(f ^ 1, facDivF, __ldg(P.chi + fc), gh.fine_ghost(V, cmp, fb, k0, q), V.v(fc, cmp),
+                           gh.fine_ghost(U, cmp, fb, k0, q), U.v(fc, cmp));
+        }
+        S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+      }
+    }
+    if (gpres) {
+      if (k == 0 && !vel) S.kind[lb][f] = gh.s.kind;
+      const Fld Q{P.pres, 1};
+      const double g = gh.value(Q, 0, false);
+      labv(S, kLabP, lb, gx, gy) = g;
+      if (gh.s.kind == kFiner) {
+        const double own = g - Q.v(gh.cell, 0);
+        int64_t fb;
+        int k0;
+        gh.fine_cells(fb, k0);
+        double fs[2];
+        for (int q = 0; q < 2; ++q) fs[q] = gh.fine_ghost(Q, 0, fb, k0, q) - Q.v(gh.fine_cell(fb, k0, q, 0), 0);
+        S.corr[1][lb][f][k] = own + (fs[0] + fs[1]);
+      }
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
+  const int along[4] = {iy, iy, ix, ix};
+  double t;
+  if (vel) {
+    const double h = cell_h(G.F, G.F.level[b]);
+    const double facDiv = 0.5 * h / dt;
+    t = facDiv * ((labv(S, kLabU, lb, ix + 1, iy) - labv(S, kLabU, lb, ix - 1, iy)) +
+                  (labv(S, kLabV, lb, ix, iy + 1) - labv(S, kLabV, lb, ix, iy - 1)));
+    t += -facDiv * chi * ((labv(S, kLabUd, lb, ix + 1, iy) - labv(S, kLabUd, lb, ix - 1, iy)) +
+                          (labv(S, kLabVd, lb, ix, iy + 1) - labv(S, kLabVd, lb, ix, iy - 1)));
+    for (int f = 0; f < 4; ++f)
+      if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[0][lb][f][along[f]];
+  } else {
+    t = P.tmp[cell];
+  }
+  if (pres) {
+    t -= ((labv(S, kLabP, lb, ix - 1, iy) + labv(S, kLabP, lb, ix + 1, iy)) +
+          (labv(S, kLabP, lb, ix, iy - 1) + labv(S, kLabP, lb, ix, iy + 1))) -
+         4.0 * p0;
+    for (int f = 0; f < 4; ++f)
+      if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[1][lb][f][along[f]];
+    P.pold[cell] = p0;
+  }
+  P.tmp[cell] = t;
+}
+
+__global__ void __launch_bounds__(kProjThreads, 4) k_pressure_correction(const __grid_constant__ Geo G, double dt,
+                                                                           const double* __restrict__ pres,
+                                                                           double* __restrict__ vel) {
+  __shared__ ProjSmem S;
+  const int lb = threadIdx.x >> 6, c = threadIdx.x & 63, ix = c & 7, iy = c >> 3;
+  const int64_t b = (int64_t)blockIdx.x * kLabBlocks + lb;
+  const bool valid = b < G.F.nb;
+  const int64_t cell = b * kBLEN + c;
+  const Fld Q{pres, 1};
+  Side sd{kEdge, -1, {-1, -1}};
+  if (valid && c < 4 * kBS) sd = G.side(b, c >> 3);  // ahead of the staging load
+  if (valid) labv(S, kLabP, lb, ix, iy) = __ldg(pres + cell);
+  if (valid && c < 4 * kBS) {
+    const Ghost gh(G, b, c, sd);
+    const int k = c & 7, f = gh.f;
+    if (k == 0) S.kind[lb][f] = gh.s.kind;
+    const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
+    const double g = gh.value(Q, 0, false);
+    labv(S, kLabP, lb, gx, gy) = g;
+    if (gh.s.kind == kFiner) {
+      const double pFac = -0.5 * dt * cell_h(G.F, G.F.level[b]);
+      const double own = grad_face(f, pFac, g, Q.v(gh.cell, 0));
+      int64_t fb;
+      int k0;
+      gh.fine_cells(fb, k0);
+      const double pFacF = -0.5 * dt * cell_h(G.F, G.F.level[fb]);
+      double fs[2];
+      for (int q = 0; q < 2; ++q)
+        fs[q] = grad_face(f ^ 1, pFacF, gh.fine_ghost(Q, 0, fb, k0, q), Q.v(gh.fine_cell(fb, k0, q, 0), 0));
+      S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  const double h = cell_h(G.F, G.F.level[b]);
+  const double pFac = -0.5 * dt * h;
+  double tv[2];
+  tv[0] = pFac * (labv(S, kLabP, lb, ix + 1, iy) - labv(S, kLabP, lb, ix - 1, iy));
+  tv[1] = pFac * (labv(S, kLabP, lb, ix, iy + 1) - labv(S, kLabP, lb, ix, iy - 1));
+  const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
+  const int along[4] = {iy, iy, ix, ix};
+  for (int f = 0; f < 4; ++f)
+    if (edge[f] && S.kind[lb][f] == kFiner) tv[f < 2 ? 0 : 1] = tv[f < 2 ? 0 : 1] + S.corr[0][lb][f][along[f]];
   const double ih2 = 1.0 / h / h;
-  vel[2 * cell] += tv[0] * ih2;
-  vel[2 * cell + 1] += tv[1] * ih2;
+  double2* v2 = reinterpret_cast<double2*>(vel) + cell;
+  double2 v = *v2;
+  v.x += tv[0] * ih2;
+  v.y += tv[1] * ih2;
+  *v2 = v;
 }
 
 }  // namespace
@@ -320,7 +410,7 @@ cudaError_t launch_pressure_rhs(const ForestView& F, const int32_t* nbr, double 
                                 cudaStream_t s) {
   const int64_t n = F.nb * kBLEN;
   if (n <= 0) return cudaSuccess;
-  k_pressure_rhs<<<(unsigned)((n + kProjThreads - 1) / kProjThreads), kProjThreads, 0, s>>>(Geo{F, nbr}, dt, f);
+  k_pressure_rhs<<<(unsigned)((F.nb + kLabBlocks - 1) / kLabBlocks), kProjThreads, 0, s>>>(Geo{F, nbr}, dt, f);
   return cudaGetLastError();
 }
 
@@ -328,8 +418,8 @@ cudaError_t launch_pressure_correction(const ForestView& F, const int32_t* nbr, 
                                        double* vel, cudaStream_t s) {
   const int64_t n = F.nb * kBLEN;
   if (n <= 0) return cudaSuccess;
-  k_pressure_correction<<<(unsigned)((n + kProjThreads - 1) / kProjThreads), kProjThreads, 0, s>>>(Geo{F, nbr}, dt,
-                                                                                                  pres, vel);
+  k_pressure_correction<<<(unsigned)((F.nb + kLabBlocks - 1) / kLabBlocks), kProjThreads, 0, s>>>(Geo{F, nbr}, dt,
+                                                                                                   pres, vel);
   return cudaGetLastError();
 }
 
