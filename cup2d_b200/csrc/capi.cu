@@ -757,6 +757,7 @@ int cup2d_poisson_pressure_rhs(cup2d_poisson* h, double dt, const double* d_vel,
   if (!h || !d_tmp || h->nb <= 0) return CUP2D_INVALID_ARGUMENT;
   if (!d_vel && !d_pres) return CUP2D_INVALID_ARGUMENT;
   if (d_vel && (!d_udef || !d_chi || !(dt > 0.0) || !std::isfinite(dt))) return CUP2D_INVALID_ARGUMENT;
+  if (d_vel && (!aligned16(d_vel) || !aligned16(d_udef))) return CUP2D_INVALID_ARGUMENT;  // 16-byte (u, v) pairs
   if (d_pres && !d_pold) return CUP2D_INVALID_ARGUMENT;
   const size_t n = (size_t)h->nb * kBLEN * sizeof(double);
   const void* bufs[6] = {d_tmp, d_pres, d_pold, d_vel, d_udef, d_chi};
@@ -775,6 +776,7 @@ int cup2d_poisson_pressure_rhs(cup2d_poisson* h, double dt, const double* d_vel,
 int cup2d_poisson_pressure_correction(cup2d_poisson* h, double dt, const double* d_pres, double* d_vel,
                                       void* stream) {
   if (!h || !d_pres || !d_vel || h->nb <= 0 || !(dt > 0.0) || !std::isfinite(dt)) return CUP2D_INVALID_ARGUMENT;
+  if (!aligned16(d_vel)) return CUP2D_INVALID_ARGUMENT;  // 16-byte (u, v) pairs
   const size_t n = (size_t)h->nb * kBLEN * sizeof(double);
   if (overlaps(d_pres, n, d_vel, 2 * n)) return CUP2D_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -36,7 +36,11 @@
 // pres (8 B) and updates vel (16 B + 16 B).  Neighbour reads hit L1/L2.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
+
 #include "kernels.hpp"
+#include "spmv.cuh"
 
 namespace cup2d {
 
@@ -75,9 +79,10 @@ struct Geo {
     return F.table[F.off[l] + j * ((int64_t)F.bpdx << l) + i];
   }
 
-  __device__ Side side(int64_t b, int f) const {
+  // The side of face f of block b from the face's neighbour table entry
+  // (nbr[4 b + f], loaded ahead by the caller).
+  __device__ Side side_from_code(int64_t b, int f, int32_t code) const {
     Side s{kEdge, -1, {-1, -1}};
-    const int32_t code = nbr[4 * b + f];
     if (code >= 0) {
       s.kind = kSame;
       s.blk = code;
@@ -248,109 +253,149 @@ __device__ __forceinline__ double& labv(ProjSmem& S, int q, int lb, int ix, int 
   return S.lab[q][lb][iy + 1][ix + 1];
 }
 
+// What one thread loads for its cell of a group of kLabBlocks blocks, one
+// group ahead of the group it computes: the staged values and, for ghost
+// threads, the face's neighbour table entry.  CTAs are persistent: each
+// walks groups blockIdx.x, + gridDim.x, ..., so the loads of the next group
+// are in flight while the ghost work and the stencil of the current one run.
+struct Prefetch {
+  double2 u, ud;
+  double chi, p;
+  int32_t code;
+};
+
+// The RHS kernel's labs, double-buffered: the next group's cells are copied
+// in with cp.async (16-byte (u, v) pairs straight into shared memory, no
+// registers held) while the current group is computed.
+struct RhsSmem {
+  double2 uv[2][kLabBlocks][kLab][kLab];  // (u, v); a face's ghost fills the normal component only
+  double2 ud[2][kLabBlocks][kLab][kLab];  // (ud, vd)
+  double p[2][kLabBlocks][kLab][kLab];
+  double chi[2][kLabBlocks][kBLEN];
+  double corr[2][kLabBlocks][4][kBS];     // finer faces: [0] divergence, [1] Laplacian
+  int kind[kLabBlocks][4];
+};
+
 __global__ void __launch_bounds__(kProjThreads, 4) k_pressure_rhs(const __grid_constant__ Geo G, double dt,
                                                                     const __grid_constant__ ProjFields P) {
-  __shared__ ProjSmem S;
+  __shared__ __align__(16) RhsSmem S;
   const int lb = threadIdx.x >> 6, c = threadIdx.x & 63, ix = c & 7, iy = c >> 3;
-  const int64_t b = (int64_t)blockIdx.x * kLabBlocks + lb;
-  const bool valid = b < G.F.nb;
-  const int64_t cell = b * kBLEN + c;
   const bool vel = P.vel != nullptr, pres = P.pres != nullptr;
   // ghost work: threads 0-31 of a block the velocity ghosts, 32-63 the
-  // pressure ghosts (ghost index c % 32); the face's side first, so that its
-  // table loads overlap the staging loads
+  // pressure ghosts (ghost index c % 32)
   const int gi = c & 31;
-  const bool gvel = c < 32 && vel, gpres = c >= 32 && pres;
-  Side sd{kEdge, -1, {-1, -1}};
-  if (valid && (gvel || gpres)) sd = G.side(b, gi >> 3);
-  // stage the block
-  double chi = 0.0, p0 = 0.0;
-  if (valid) {
+  const bool gvel = c < 32 && vel, gpres = c >= 32 && pres, gthr = gvel || gpres;
+  const int64_t ngroups = (G.F.nb + kLabBlocks - 1) / kLabBlocks;
+  // copies of group grp's cells into buffer q, and the face's table entry
+  auto issue = [&](int64_t grp, int q, int32_t& code) {
+    const int64_t b = grp * kLabBlocks + lb;
+    if (b >= G.F.nb) return;
+    const int64_t cell = b * kBLEN + c;
     if (vel) {
-      const double2 u = __ldg(reinterpret_cast<const double2*>(P.vel) + cell);
-      const double2 ud = __ldg(reinterpret_cast<const double2*>(P.udef) + cell);
-      chi = __ldg(P.chi + cell);
-      labv(S, kLabU, lb, ix, iy) = u.x;
-      labv(S, kLabV, lb, ix, iy) = u.y;
-      labv(S, kLabUd, lb, ix, iy) = ud.x;
-      labv(S, kLabVd, lb, ix, iy) = ud.y;
+      cp_async_n<16>(&S.uv[q][lb][iy + 1][ix + 1], P.vel + 2 * cell, 16);
+      cp_async_n<16>(&S.ud[q][lb][iy + 1][ix + 1], P.udef + 2 * cell, 16);
+      cp_async_n<8>(&S.chi[q][lb][c], P.chi + cell, 8);
     }
-    if (pres) {
-      p0 = __ldg(P.pres + cell);
-      labv(S, kLabP, lb, ix, iy) = p0;
-    }
-  }
-  // ghost layer and flux-correction terms
-  if (valid && (gvel || gpres)) {
-    const Ghost gh(G, b, gi, sd);
-    const int k = gi & 7, f = gh.f;
-    if (k == 0 && c < 32) S.kind[lb][f] = gh.s.kind;
-    const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
-    const double h = cell_h(G.F, G.F.level[b]);
-    if (gvel) {
-      const Fld V{P.vel, 2}, U{P.udef, 2};
-      const int cmp = gh.xface() ? 0 : 1;  // the normal component: the only one the divergence reads
-      const double g = gh.value(V, cmp, true), gd = gh.value(U, cmp, true);
-      labv(S, gh.xface() ? kLabU : kLabV, lb, gx, gy) = g;
-      labv(S, gh.xface() ? kLabUd : kLabVd, lb, gx, gy) = gd;
-      if (gh.s.kind == kFiner) {
-        const double facDiv = 0.5 * h / dt;
-        const double own = div_face(f, facDiv, __ldg(P.chi + gh.cell), g, V.v(gh.cell, cmp), gd, U.v(gh.cell, cmp));
-        int64_t fb;
-        int k0;
-        gh.fine_cells(fb, k0);
-        const double facDivF = 0.5 * cell_h(G.F, G.F.level[fb]) / dt;
-        double fs[2];
-        for (int q = 0; q < 2; ++q) {
-          const int64_t fc = gh.fine_cell(fb, k0, q, 0);
-          fs[q] = div_face(f ^ 1, facDivF, __ldg(P.chi + fc), gh.fine_ghost(V, cmp, fb, k0, q), V.v(fc, cmp),
-                           gh.fine_ghost(U, cmp, fb, k0, q), U.v(fc, cmp));
+    if (pres) cp_async_n<8>(&S.p[q][lb][iy + 1][ix + 1], P.pres + cell, 8);
+    if (gthr) code = __ldg(G.nbr + 4 * b + (gi >> 3));
+  };
+  int32_t code = 0, code_next = 0;
+  int64_t grp = blockIdx.x;
+  if (grp < ngroups) issue(grp, 0, code);
+  cp_async_commit_group();
+  for (int it = 0; grp < ngroups; grp += gridDim.x, ++it) {
+    const int q = it & 1;
+    cp_async_wait_n<0>();  // this group's cells have landed (every thread's, after the barrier)
+    __syncthreads();
+    if (grp + gridDim.x < ngroups) issue(grp + gridDim.x, q ^ 1, code_next);
+    cp_async_commit_group();
+    const int64_t b = grp * kLabBlocks + lb;
+    const bool valid = b < G.F.nb;
+    const int64_t cell = b * kBLEN + c;
+    // ghost layer and flux-correction terms
+    if (valid && gthr) {
+      const Ghost gh(G, b, gi, G.side_from_code(b, gi >> 3, code));
+      const int k = gi & 7, f = gh.f;
+      if (k == 0 && (c < 32 || !vel)) S.kind[lb][f] = gh.s.kind;
+      const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
+      const double h = cell_h(G.F, G.F.level[b]);
+      if (gvel) {
+        const Fld V{P.vel, 2}, U{P.udef, 2};
+        const int cmp = gh.xface() ? 0 : 1;  // the normal component: the only one the divergence reads
+        const double g = gh.value(V, cmp, true), gd = gh.value(U, cmp, true);
+        if (cmp == 0) {
+          S.uv[q][lb][gy + 1][gx + 1].x = g;
+          S.ud[q][lb][gy + 1][gx + 1].x = gd;
+        } else {
+          S.uv[q][lb][gy + 1][gx + 1].y = g;
+          S.ud[q][lb][gy + 1][gx + 1].y = gd;
         }
-        S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+        if (gh.s.kind == kFiner) {
+          const double facDiv = 0.5 * h / dt;
+          const double own =
+              div_face(f, facDiv, __ldg(P.chi + gh.cell), g, V.v(gh.cell, cmp), gd, U.v(gh.cell, cmp));
+          int64_t fb;
+          int k0;
+          gh.fine_cells(fb, k0);
+          const double facDivF = 0.5 * cell_h(G.F, G.F.level[fb]) / dt;
+          double fs[2];
+          for (int r = 0; r < 2; ++r) {
+            const int64_t fc = gh.fine_cell(fb, k0, r, 0);
+            fs[r] = div_face(f ^ 1, facDivF, __ldg(P.chi + fc), gh.fine_ghost(V, cmp, fb, k0, r), V.v(fc, cmp),
+                             gh.fine_ghost(U, cmp, fb, k0, r), U.v(fc, cmp));
+          }
+          S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+        }
+      }
+      if (gpres) {
+        const Fld Q{P.pres, 1};
+        const double g = gh.value(Q, 0, false);
+        S.p[q][lb][gy + 1][gx + 1] = g;
+        if (gh.s.kind == kFiner) {
+          const double own = g - Q.v(gh.cell, 0);
+          int64_t fb;
+          int k0;
+          gh.fine_cells(fb, k0);
+          double fs[2];
+          for (int r = 0; r < 2; ++r) fs[r] = gh.fine_ghost(Q, 0, fb, k0, r) - Q.v(gh.fine_cell(fb, k0, r, 0), 0);
+          S.corr[1][lb][f][k] = own + (fs[0] + fs[1]);
+        }
       }
     }
-    if (gpres) {
-      if (k == 0 && !vel) S.kind[lb][f] = gh.s.kind;
-      const Fld Q{P.pres, 1};
-      const double g = gh.value(Q, 0, false);
-      labv(S, kLabP, lb, gx, gy) = g;
-      if (gh.s.kind == kFiner) {
-        const double own = g - Q.v(gh.cell, 0);
-        int64_t fb;
-        int k0;
-        gh.fine_cells(fb, k0);
-        double fs[2];
-        for (int q = 0; q < 2; ++q) fs[q] = gh.fine_ghost(Q, 0, fb, k0, q) - Q.v(gh.fine_cell(fb, k0, q, 0), 0);
-        S.corr[1][lb][f][k] = own + (fs[0] + fs[1]);
+    __syncthreads();
+    if (valid) {
+      const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
+      const int along[4] = {iy, iy, ix, ix};
+      const int X = ix + 1, Y = iy + 1;
+      double t;
+      if (vel) {
+        const double h = cell_h(G.F, G.F.level[b]);
+        const double facDiv = 0.5 * h / dt;
+        const double chi = S.chi[q][lb][c];
+        t = facDiv * ((S.uv[q][lb][Y][X + 1].x - S.uv[q][lb][Y][X - 1].x) +
+                      (S.uv[q][lb][Y + 1][X].y - S.uv[q][lb][Y - 1][X].y));
+        t += -facDiv * chi * ((S.ud[q][lb][Y][X + 1].x - S.ud[q][lb][Y][X - 1].x) +
+                              (S.ud[q][lb][Y + 1][X].y - S.ud[q][lb][Y - 1][X].y));
+        for (int f = 0; f < 4; ++f)
+          if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[0][lb][f][along[f]];
+      } else {
+        t = P.tmp[cell];
       }
+      if (pres) {
+        const double p0 = S.p[q][lb][Y][X];
+        t -= ((S.p[q][lb][Y][X - 1] + S.p[q][lb][Y][X + 1]) + (S.p[q][lb][Y - 1][X] + S.p[q][lb][Y + 1][X])) -
+             4.0 * p0;
+        for (int f = 0; f < 4; ++f)
+          if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[1][lb][f][along[f]];
+        P.pold[cell] = p0;
+      }
+      P.tmp[cell] = t;
     }
+    code = code_next;
+    // the next iteration's first barrier orders these reads of buffer q
+    // before that iteration's copies into it
   }
-  __syncthreads();
-  if (!valid) return;
-  const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
-  const int along[4] = {iy, iy, ix, ix};
-  double t;
-  if (vel) {
-    const double h = cell_h(G.F, G.F.level[b]);
-    const double facDiv = 0.5 * h / dt;
-    t = facDiv * ((labv(S, kLabU, lb, ix + 1, iy) - labv(S, kLabU, lb, ix - 1, iy)) +
-                  (labv(S, kLabV, lb, ix, iy + 1) - labv(S, kLabV, lb, ix, iy - 1)));
-    t += -facDiv * chi * ((labv(S, kLabUd, lb, ix + 1, iy) - labv(S, kLabUd, lb, ix - 1, iy)) +
-                          (labv(S, kLabVd, lb, ix, iy + 1) - labv(S, kLabVd, lb, ix, iy - 1)));
-    for (int f = 0; f < 4; ++f)
-      if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[0][lb][f][along[f]];
-  } else {
-    t = P.tmp[cell];
-  }
-  if (pres) {
-    t -= ((labv(S, kLabP, lb, ix - 1, iy) + labv(S, kLabP, lb, ix + 1, iy)) +
-          (labv(S, kLabP, lb, ix, iy - 1) + labv(S, kLabP, lb, ix, iy + 1))) -
-         4.0 * p0;
-    for (int f = 0; f < 4; ++f)
-      if (edge[f] && S.kind[lb][f] == kFiner) t = t + S.corr[1][lb][f][along[f]];
-    P.pold[cell] = p0;
-  }
-  P.tmp[cell] = t;
+  cp_async_wait_n<0>();  // nothing may land after return
 }
 
 __global__ void __launch_bounds__(kProjThreads, 4) k_pressure_correction(const __grid_constant__ Geo G, double dt,
@@ -358,68 +403,102 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_pressure_correction(const _
                                                                            double* __restrict__ vel) {
   __shared__ ProjSmem S;
   const int lb = threadIdx.x >> 6, c = threadIdx.x & 63, ix = c & 7, iy = c >> 3;
-  const int64_t b = (int64_t)blockIdx.x * kLabBlocks + lb;
-  const bool valid = b < G.F.nb;
-  const int64_t cell = b * kBLEN + c;
+  const bool gthr = c < 4 * kBS;
   const Fld Q{pres, 1};
-  Side sd{kEdge, -1, {-1, -1}};
-  if (valid && c < 4 * kBS) sd = G.side(b, c >> 3);  // ahead of the staging load
-  if (valid) labv(S, kLabP, lb, ix, iy) = __ldg(pres + cell);
-  if (valid && c < 4 * kBS) {
-    const Ghost gh(G, b, c, sd);
-    const int k = c & 7, f = gh.f;
-    if (k == 0) S.kind[lb][f] = gh.s.kind;
-    const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
-    const double g = gh.value(Q, 0, false);
-    labv(S, kLabP, lb, gx, gy) = g;
-    if (gh.s.kind == kFiner) {
-      const double pFac = -0.5 * dt * cell_h(G.F, G.F.level[b]);
-      const double own = grad_face(f, pFac, g, Q.v(gh.cell, 0));
-      int64_t fb;
-      int k0;
-      gh.fine_cells(fb, k0);
-      const double pFacF = -0.5 * dt * cell_h(G.F, G.F.level[fb]);
-      double fs[2];
-      for (int q = 0; q < 2; ++q)
-        fs[q] = grad_face(f ^ 1, pFacF, gh.fine_ghost(Q, 0, fb, k0, q), Q.v(gh.fine_cell(fb, k0, q, 0), 0));
-      S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+  const int64_t ngroups = (G.F.nb + kLabBlocks - 1) / kLabBlocks;
+  auto fetch = [&](int64_t grp, Prefetch& q) {
+    const int64_t b = grp * kLabBlocks + lb;
+    if (b >= G.F.nb) return;
+    const int64_t cell = b * kBLEN + c;
+    q.p = __ldg(pres + cell);
+    q.u = reinterpret_cast<const double2*>(vel)[cell];  // updated in place: no read-only path
+    if (gthr) q.code = __ldg(G.nbr + 4 * b + (c >> 3));
+  };
+  Prefetch cur{}, nxt{};
+  int64_t grp = blockIdx.x;
+  if (grp < ngroups) fetch(grp, cur);
+  for (; grp < ngroups; grp += gridDim.x) {
+    const int64_t b = grp * kLabBlocks + lb;
+    const bool valid = b < G.F.nb;
+    const int64_t cell = b * kBLEN + c;
+    if (valid) labv(S, kLabP, lb, ix, iy) = cur.p;
+    if (grp + gridDim.x < ngroups) fetch(grp + gridDim.x, nxt);
+    if (valid && gthr) {
+      const Ghost gh(G, b, c, G.side_from_code(b, c >> 3, cur.code));
+      const int k = c & 7, f = gh.f;
+      if (k == 0) S.kind[lb][f] = gh.s.kind;
+      const int gx = gh.ix + (f == 0 ? -1 : f == 1 ? 1 : 0), gy = gh.iy + (f == 2 ? -1 : f == 3 ? 1 : 0);
+      const double g = gh.value(Q, 0, false);
+      labv(S, kLabP, lb, gx, gy) = g;
+      if (gh.s.kind == kFiner) {
+        const double pFac = -0.5 * dt * cell_h(G.F, G.F.level[b]);
+        const double own = grad_face(f, pFac, g, Q.v(gh.cell, 0));
+        int64_t fb;
+        int k0;
+        gh.fine_cells(fb, k0);
+        const double pFacF = -0.5 * dt * cell_h(G.F, G.F.level[fb]);
+        double fs[2];
+        for (int q = 0; q < 2; ++q)
+          fs[q] = grad_face(f ^ 1, pFacF, gh.fine_ghost(Q, 0, fb, k0, q), Q.v(gh.fine_cell(fb, k0, q, 0), 0));
+        S.corr[0][lb][f][k] = own + (fs[0] + fs[1]);
+      }
     }
+    __syncthreads();
+    if (valid) {
+      const double h = cell_h(G.F, G.F.level[b]);
+      const double pFac = -0.5 * dt * h;
+      double tv[2];
+      tv[0] = pFac * (labv(S, kLabP, lb, ix + 1, iy) - labv(S, kLabP, lb, ix - 1, iy));
+      tv[1] = pFac * (labv(S, kLabP, lb, ix, iy + 1) - labv(S, kLabP, lb, ix, iy - 1));
+      const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
+      const int along[4] = {iy, iy, ix, ix};
+      for (int f = 0; f < 4; ++f)
+        if (edge[f] && S.kind[lb][f] == kFiner) tv[f < 2 ? 0 : 1] = tv[f < 2 ? 0 : 1] + S.corr[0][lb][f][along[f]];
+      const double ih2 = 1.0 / h / h;
+      double2 v = cur.u;
+      v.x += tv[0] * ih2;
+      v.y += tv[1] * ih2;
+      reinterpret_cast<double2*>(vel)[cell] = v;
+    }
+    __syncthreads();
+    cur = nxt;
   }
-  __syncthreads();
-  if (!valid) return;
-  const double h = cell_h(G.F, G.F.level[b]);
-  const double pFac = -0.5 * dt * h;
-  double tv[2];
-  tv[0] = pFac * (labv(S, kLabP, lb, ix + 1, iy) - labv(S, kLabP, lb, ix - 1, iy));
-  tv[1] = pFac * (labv(S, kLabP, lb, ix, iy + 1) - labv(S, kLabP, lb, ix, iy - 1));
-  const bool edge[4] = {ix == 0, ix == kBS - 1, iy == 0, iy == kBS - 1};
-  const int along[4] = {iy, iy, ix, ix};
-  for (int f = 0; f < 4; ++f)
-    if (edge[f] && S.kind[lb][f] == kFiner) tv[f < 2 ? 0 : 1] = tv[f < 2 ? 0 : 1] + S.corr[0][lb][f][along[f]];
-  const double ih2 = 1.0 / h / h;
-  double2* v2 = reinterpret_cast<double2*>(vel) + cell;
-  double2 v = *v2;
-  v.x += tv[0] * ih2;
-  v.y += tv[1] * ih2;
-  *v2 = v;
+}
+
+// Persistent grid: the co-resident CTAs of a kernel (queried once per device).
+int persistent_grid(const void* fn, int which, int64_t ngroups) {
+  static std::atomic<int> cap[64][2];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  int g = cap[dev][which].load(std::memory_order_acquire);
+  if (g <= 0) {
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kProjThreads, 0) != cudaSuccess)
+      return 0;
+    g = std::max(1, sms * per_sm);
+    cap[dev][which].store(g, std::memory_order_release);
+  }
+  return (int)std::min<int64_t>(g, ngroups);
 }
 
 }  // namespace
 
 cudaError_t launch_pressure_rhs(const ForestView& F, const int32_t* nbr, double dt, const ProjFields& f,
                                 cudaStream_t s) {
-  const int64_t n = F.nb * kBLEN;
-  if (n <= 0) return cudaSuccess;
-  k_pressure_rhs<<<(unsigned)((F.nb + kLabBlocks - 1) / kLabBlocks), kProjThreads, 0, s>>>(Geo{F, nbr}, dt, f);
+  if (F.nb <= 0) return cudaSuccess;
+  const int grid = persistent_grid((const void*)k_pressure_rhs, 0, (F.nb + kLabBlocks - 1) / kLabBlocks);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  k_pressure_rhs<<<grid, kProjThreads, 0, s>>>(Geo{F, nbr}, dt, f);
   return cudaGetLastError();
 }
 
 cudaError_t launch_pressure_correction(const ForestView& F, const int32_t* nbr, double dt, const double* pres,
                                        double* vel, cudaStream_t s) {
-  const int64_t n = F.nb * kBLEN;
-  if (n <= 0) return cudaSuccess;
-  k_pressure_correction<<<(unsigned)((F.nb + kLabBlocks - 1) / kLabBlocks), kProjThreads, 0, s>>>(Geo{F, nbr}, dt,
-                                                                                                   pres, vel);
+  if (F.nb <= 0) return cudaSuccess;
+  const int grid = persistent_grid((const void*)k_pressure_correction, 1, (F.nb + kLabBlocks - 1) / kLabBlocks);
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  k_pressure_correction<<<grid, kProjThreads, 0, s>>>(Geo{F, nbr}, dt, pres, vel);
   return cudaGetLastError();
 }
 

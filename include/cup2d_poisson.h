@@ -219,7 +219,8 @@ int cup2d_poisson_pressure_step(cup2d_poisson* h, double* d_tmp, double* d_pres,
  * PressureSingle.cpp), on device buffers in block-major cell order.
  * Velocity-like fields hold (u, v) per cell, interleaved (Cubism's
  * VectorBlock layout), scalars one double per cell; each buffer holds the
- * handle's ncells cells.  Ghost cells follow CUP2D's labs: same-level
+ * handle's ncells cells; velocity-like buffers 16-byte aligned (cudaMalloc
+ * gives 256).  Ghost cells follow CUP2D's labs: same-level
  * neighbours, domain edges (velocities: normal component sign-flipped;
  * scalars: copied), coarser neighbours by the operator's quadratic
  * interpolation (ExpAMRSolver.cpp:100-128), and coarse cells next to finer
