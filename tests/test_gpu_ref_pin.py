@@ -187,14 +187,15 @@ def test_server_large_request_alone_equals_in_mix(cuda):
     assert big.nblocks >= 10000
     small = [small_mesh(), sized_mesh(rng, 300), sized_mesh(rng, 900)]
     meshes = [big] + small
-    with Server(max_inflight=8, team=0, tol_rel=1e-6, max_iter=5000, precision="mixed") as S:
+    bpc = 320  # blocks per CTA of a served solve's team
+    with Server(max_inflight=8, team=0, blocks_per_cta=bpc, tol_rel=1e-6, max_iter=5000, precision="mixed") as S:
         ids = [S.add_mesh(m) for m in meshes]
         reqs = [(k, meshes[k].rhs_fourier(500 + j)) for j in range(3) for k in range(len(meshes))]
         xs = [np.zeros_like(b) for _, b in reqs]
         rids = [S.submit(ids[k], b, x) for (k, b), x in zip(reqs, xs)]
         stats = [S.wait(r, timeout_ms=120000) for r in rids]
     assert all(s is not None and s["status"] == L.OK for s in stats), stats
-    team = min(128, max(2, (big.nblocks + 80) // 160))
+    team = min(128, max(2, (big.nblocks + bpc // 2) // bpc))
     for (k, b), x in zip(reqs, xs):
         if k != 0:
             continue
