@@ -1079,7 +1079,7 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_bat
   batch_body<false>(A);
 }
 
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch_mixed(const __grid_constant__ BatchArgs A) {
+__global__ void __launch_bounds__(kSolveThreads, kBatchMixedCtasPerSm) k_bicgstab_batch_mixed(const __grid_constant__ BatchArgs A) {
   batch_body<true>(A);
 }
 
@@ -1114,7 +1114,8 @@ cudaError_t allow_smem(const void* fn) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
   if (e == cudaSuccess && per_sm > 0) {
-    const size_t need = (size_t)kSolveCtasPerSm * (bytes + (size_t)reserved);
+    const int ctas = fn == kSolveFns[3] ? kBatchMixedCtasPerSm : kSolveCtasPerSm;  // [3]: the mixed batch
+    const size_t need = (size_t)ctas * (bytes + (size_t)reserved);
     const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / (size_t)per_sm);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
   }

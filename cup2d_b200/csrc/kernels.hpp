@@ -171,6 +171,14 @@ constexpr int kSolveThreads = 256;
 #define CUP2D_CTAS_PER_SM 3
 #endif
 constexpr int kSolveCtasPerSm = CUP2D_CTAS_PER_SM;
+// The mixed batch kernel: 2 CTAs per SM (128 registers, no spills).  Measured
+// on the 512-problem batch, same box, one build against the other: 806-808
+// solves/s against 781 at 3 CTAs per SM (team 6 against 8); the FP64 batch
+// lost 8.5 % the same way, so it stays at 3.
+#ifndef CUP2D_BATCH_MIXED_CTAS_PER_SM
+#define CUP2D_BATCH_MIXED_CTAS_PER_SM 2
+#endif
+constexpr int kBatchMixedCtasPerSm = CUP2D_BATCH_MIXED_CTAS_PER_SM;
 
 // Largest co-resident grid of the persistent kernels on this device.
 int max_coop_grid_fp64(int device);
