@@ -1075,7 +1075,7 @@ __device__ __forceinline__ void batch_body(const BatchArgs& A) {
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_batch64(const __grid_constant__ BatchArgs A) {
+__global__ void __launch_bounds__(kSolveThreads, kBatch64CtasPerSm) k_bicgstab_batch64(const __grid_constant__ BatchArgs A) {
   batch_body<false>(A);
 }
 
@@ -1097,7 +1097,8 @@ size_t smem_bytes(const void* fn) {
 
 // Allows the dynamic shared memory of a solve kernel on the current device
 // (once per device and kernel) and asks for the smallest shared-memory
-// carve-out that holds kSolveCtasPerSm of its CTAs, so that the rest of the
+// carve-out that holds its CTAs per SM (kSolveCtasPerSm, or the batch
+// kernels' own counts), so that the rest of the
 // unified array stays L1.
 cudaError_t allow_smem(const void* fn) {
   static unsigned done[64] = {};
@@ -1114,7 +1115,9 @@ cudaError_t allow_smem(const void* fn) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
   if (e == cudaSuccess && per_sm > 0) {
-    const int ctas = fn == kSolveFns[3] ? kBatchMixedCtasPerSm : kSolveCtasPerSm;  // [3]: the mixed batch
+    const int ctas = fn == kSolveFns[3] ? kBatchMixedCtasPerSm  // [3]: the mixed batch
+                     : fn == kSolveFns[2] ? kBatch64CtasPerSm    // [2]: the FP64 batch
+                                          : kSolveCtasPerSm;
     const size_t need = (size_t)ctas * (bytes + (size_t)reserved);
     const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / (size_t)per_sm);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);

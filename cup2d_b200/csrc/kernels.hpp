@@ -179,6 +179,10 @@ constexpr int kSolveCtasPerSm = CUP2D_CTAS_PER_SM;
 #define CUP2D_BATCH_MIXED_CTAS_PER_SM 2
 #endif
 constexpr int kBatchMixedCtasPerSm = CUP2D_BATCH_MIXED_CTAS_PER_SM;
+#ifndef CUP2D_BATCH64_CTAS_PER_SM
+#define CUP2D_BATCH64_CTAS_PER_SM 3
+#endif
+constexpr int kBatch64CtasPerSm = CUP2D_BATCH64_CTAS_PER_SM;
 
 // Largest co-resident grid of the persistent kernels on this device.
 int max_coop_grid_fp64(int device);
