@@ -965,9 +965,11 @@ __device__ __forceinline__ Smem<T>& solve_smem() {
 
 // ====================================================== single solves =====
 
-// Three CTAs per SM (80 registers): the passes are bound by per-warp memory
-// latency, and the extra warps outweigh the spills this costs (measured on
-// the large workload: 2/3/4 CTAs per SM gave 97/95/104 us per iteration).
+// kSolveCtasPerSm CTAs per SM (2: up to 128 registers, no spills).  With the
+// SpMV operands staged in shared memory the spill-free build gained 6-7 % per
+// iteration on the large workload and ~10 % on time stepping over 3 CTAs at
+// 80 registers (an earlier kernel, gathering its operands into registers,
+// had measured 97/95/104 us per iteration at 2/3/4).
 __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab64(const __grid_constant__ SolveArgs64 S) {
   Smem<double>& sm = solve_smem<double>();
   const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
@@ -1016,6 +1018,40 @@ __global__ void __launch_bounds__(kSolveThreads, kSolveCtasPerSm) k_bicgstab_mix
   solve_mixed(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
 }
 
+
+// The server's instances of the two single solves: the same bodies at
+// kServedCtasPerSm CTAs per SM.
+__global__ void __launch_bounds__(kSolveThreads, kServedCtasPerSm)
+    k_bicgstab64_served(const __grid_constant__ SolveArgs64 S) {
+  Smem<double>& sm = solve_smem<double>();
+  const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
+  if (threadIdx.x == 0) {
+    sm.team_rank = blockIdx.x;
+    sm.team_size = gridDim.x;
+  }
+  Pinv<double> pin;
+  pin.load(sm.P, S.P, nullptr);
+  __syncthreads();
+  solve_fp64<false>(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
+}
+
+__global__ void __launch_bounds__(kSolveThreads, kServedCtasPerSm)
+    k_bicgstab_mixed_served(const __grid_constant__ SolveArgsMixed S) {
+  Smem<float>& sm = solve_smem<float>();
+  const int b0 = share(S.prob.M.nb, blockIdx.x, gridDim.x), b1 = share(S.prob.M.nb, blockIdx.x + 1, gridDim.x);
+  const int r0 = share(S.prob.M.R, blockIdx.x, gridDim.x), r1 = share(S.prob.M.R, blockIdx.x + 1, gridDim.x);
+  GridBarrier B{S.bar, S.abort_flag, gridDim.x, globaltimer_ns() + S.timeout_ns, 0u, S.prof, globaltimer_ns()};
+  if (threadIdx.x == 0) {
+    sm.team_rank = blockIdx.x;
+    sm.team_size = gridDim.x;
+  }
+  Pinv<float> pin;
+  pin.load(sm.P, nullptr, S.P32);
+  __syncthreads();
+  solve_mixed(sm, B, pin, S.prob, S.sp, S.red, b0, b1, r0, r1);
+}
 
 // ========================================================= batches ========
 //
@@ -1086,19 +1122,24 @@ __global__ void __launch_bounds__(kSolveThreads, kBatchMixedCtasPerSm) k_bicgsta
 // ------------------------------------------------------------ launch -----
 
 namespace {
-constexpr int kNumSolveFns = 5;
-const void* const kSolveFns[kNumSolveFns] = {(const void*)k_bicgstab64, (const void*)k_bicgstab_mixed,
-                                             (const void*)k_bicgstab_batch64, (const void*)k_bicgstab_batch_mixed,
-                                             (const void*)k_bicgstab64_mean};
+constexpr int kNumSolveFns = 7;
+const void* const kSolveFns[kNumSolveFns] = {(const void*)k_bicgstab64,        (const void*)k_bicgstab_mixed,
+                                             (const void*)k_bicgstab_batch64,  (const void*)k_bicgstab_batch_mixed,
+                                             (const void*)k_bicgstab64_mean,   (const void*)k_bicgstab64_served,
+                                             (const void*)k_bicgstab_mixed_served};
+// CTAs per SM each kernel is built for
+const int kSolveFnCtas[kNumSolveFns] = {kSolveCtasPerSm,  kSolveCtasPerSm,  kBatch64CtasPerSm, kBatchMixedCtasPerSm,
+                                        kSolveCtasPerSm,  kServedCtasPerSm, kServedCtasPerSm};
 
 size_t smem_bytes(const void* fn) {
-  return (fn == kSolveFns[1] || fn == kSolveFns[3]) ? sizeof(Smem<float>) : sizeof(Smem<double>);
+  return (fn == kSolveFns[1] || fn == kSolveFns[3] || fn == kSolveFns[6]) ? sizeof(Smem<float>)
+                                                                           : sizeof(Smem<double>);
 }
 
 // Allows the dynamic shared memory of a solve kernel on the current device
 // (once per device and kernel) and asks for the smallest shared-memory
-// carve-out that holds its CTAs per SM (kSolveCtasPerSm, or the batch
-// kernels' own counts), so that the rest of the
+// carve-out that holds the CTAs per SM it is built for (kSolveFnCtas), so
+// that the rest of the
 // unified array stays L1.
 cudaError_t allow_smem(const void* fn) {
   static unsigned done[64] = {};
@@ -1115,9 +1156,7 @@ cudaError_t allow_smem(const void* fn) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
   if (e == cudaSuccess && per_sm > 0) {
-    const int ctas = fn == kSolveFns[3] ? kBatchMixedCtasPerSm  // [3]: the mixed batch
-                     : fn == kSolveFns[2] ? kBatch64CtasPerSm    // [2]: the FP64 batch
-                                          : kSolveCtasPerSm;
+    const int ctas = k < kNumSolveFns ? kSolveFnCtas[k] : kSolveCtasPerSm;
     const size_t need = (size_t)ctas * (bytes + (size_t)reserved);
     const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / (size_t)per_sm);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
@@ -1153,24 +1192,30 @@ int coop_grid(const void* fn, int device) {
 }
 }  // namespace
 
-int max_coop_grid_fp64(int device) { return coop_grid((const void*)k_bicgstab64, device); }
-int max_coop_grid_mixed(int device) { return coop_grid((const void*)k_bicgstab_mixed, device); }
+int max_coop_grid_fp64(int device, bool served) {
+  return coop_grid(served ? (const void*)k_bicgstab64_served : (const void*)k_bicgstab64, device);
+}
+int max_coop_grid_mixed(int device, bool served) {
+  return coop_grid(served ? (const void*)k_bicgstab_mixed_served : (const void*)k_bicgstab_mixed, device);
+}
 
 int max_coop_grid_mean(int device) { return coop_grid((const void*)k_bicgstab64_mean, device); }
 
-cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s) {
+cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s, bool served) {
   void* args[] = {const_cast<SolveArgs64*>(&a)};
-  const void* fn = a.sp.mean_row >= 0 ? (const void*)k_bicgstab64_mean : (const void*)k_bicgstab64;
+  const void* fn = a.sp.mean_row >= 0 ? (const void*)k_bicgstab64_mean
+                   : served           ? (const void*)k_bicgstab64_served
+                                      : (const void*)k_bicgstab64;
   if (cudaError_t e = allow_smem(fn)) return e;
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolveThreads), args, sizeof(Smem<double>), s);
 }
 
-cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s) {
+cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s, bool served) {
   void* args[] = {const_cast<SolveArgsMixed*>(&a)};
   if (a.sp.mean_row >= 0) return cudaErrorInvalidValue;  // FP64 only
-  if (cudaError_t e = allow_smem((const void*)k_bicgstab_mixed)) return e;
-  return cudaLaunchCooperativeKernel((const void*)k_bicgstab_mixed, dim3(grid), dim3(kSolveThreads), args,
-                                     sizeof(Smem<float>), s);
+  const void* fn = served ? (const void*)k_bicgstab_mixed_served : (const void*)k_bicgstab_mixed;
+  if (cudaError_t e = allow_smem(fn)) return e;
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kSolveThreads), args, sizeof(Smem<float>), s);
 }
 
 int max_coop_grid_batch(int device, bool mixed) {

@@ -158,6 +158,7 @@ struct cup2d_poisson {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool owns_stream = true;  // false for the problems of a batch (batch stream)
+  bool served = false;      // a server's handle: its solves run the served kernel instances
   cup2d_solve_opts opts{};
   // forest
   int32_t bpdx = 0, bpdy = 0, level_max = 0, px = 0, py = 0;
@@ -403,14 +404,14 @@ int cup2d_pinv(double* P_out) {
 }
 
 int cup2d_poisson_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cup2d_poisson** out) {
-  return handle_create(forest, opts, nullptr, out);
+  return handle_create(forest, opts, nullptr, false, out);
 }
 
 }  // extern "C"
 
 namespace cup2d {
 
-int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cudaStream_t stream,
+int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cudaStream_t stream, bool served,
                   cup2d_poisson** out) {
   if (!out) return CUP2D_INVALID_ARGUMENT;
   *out = nullptr;
@@ -445,8 +446,9 @@ int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cuda
       return CUP2D_CUDA_ERROR;
     }
   }
-  h->grid64 = max_coop_grid_fp64(h->device);
-  h->gridmx = max_coop_grid_mixed(h->device);
+  h->served = served;
+  h->grid64 = max_coop_grid_fp64(h->device, served);
+  h->gridmx = max_coop_grid_mixed(h->device, served);
   h->grid64m = std::min(h->grid64, max_coop_grid_mean(h->device));
   if (h->grid64 <= 0 || h->gridmx <= 0) {
     cup2d_poisson_destroy(h);
@@ -652,7 +654,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
                        o.reliable_restart, mean_row};
     a.timeout_ns = tns;
     a.prof = prof;
-    e = launch_bicgstab_mixed(a, grid, s);
+    e = launch_bicgstab_mixed(a, grid, s, h->served);
   } else {
     if ((st = ensure_fp64(h))) return st;
     SolveArgs64 a{};
@@ -665,7 +667,7 @@ int cup2d_poisson_solve_device(cup2d_poisson* h, const double* d_b, double* d_x,
     a.sp = SolveParams{o.tol_abs, o.tol_rel, 0.0, o.max_restarts, o.max_iter, o.subtract_mean, 0, mean_row};
     a.timeout_ns = tns;
     a.prof = prof;
-    e = launch_bicgstab64(a, grid, s);
+    e = launch_bicgstab64(a, grid, s, h->served);
   }
   if (e != cudaSuccess) return from_cuda(e);
   if (!stats) return CUP2D_OK;

@@ -24,8 +24,9 @@ int handle_view(const cup2d_poisson* h, HandleView* out);
 
 // cup2d_poisson_create on the caller's stream: the handle assembles and runs
 // its host-buffer work there and owns no stream (the stream must outlive the
-// handle); its timing events are made on first use.
-int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cudaStream_t stream,
+// handle); its timing events are made on first use.  `served`: its solves
+// run the server's kernel instances (kServedCtasPerSm).
+int handle_create(const cup2d_forest* forest, const cup2d_solve_opts* opts, cudaStream_t stream, bool served,
                   cup2d_poisson** out);
 
 // For the request server (server.cpp).

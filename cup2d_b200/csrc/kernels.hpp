@@ -167,10 +167,20 @@ struct BatchArgs {
 };
 
 constexpr int kSolveThreads = 256;
+// CTAs per SM of the persistent kernels (launch bounds and shared-memory
+// carve-out).  Single solves run 2 (128 registers): against 3 (80 registers,
+// spilling), on one box, time stepping 16.3 -> 18.3 solves/s (mixed) and
+// 19.0 -> 21.0 (FP64), the plain FP64 loop +9 %.  The server's solves run
+// their own instances at 3: many small teams in flight need the CTA slots
+// (at 2 the server saturated at 95-113 solves/s against 127).
 #ifndef CUP2D_CTAS_PER_SM
-#define CUP2D_CTAS_PER_SM 3
+#define CUP2D_CTAS_PER_SM 2
 #endif
 constexpr int kSolveCtasPerSm = CUP2D_CTAS_PER_SM;
+#ifndef CUP2D_SERVED_CTAS_PER_SM
+#define CUP2D_SERVED_CTAS_PER_SM 3
+#endif
+constexpr int kServedCtasPerSm = CUP2D_SERVED_CTAS_PER_SM;
 // The mixed batch kernel: 2 CTAs per SM (128 registers, no spills).  Measured
 // on the 512-problem batch, same box, one build against the other: 806-808
 // solves/s against 781 at 3 CTAs per SM (team 6 against 8); the FP64 batch
@@ -185,12 +195,13 @@ constexpr int kBatchMixedCtasPerSm = CUP2D_BATCH_MIXED_CTAS_PER_SM;
 constexpr int kBatch64CtasPerSm = CUP2D_BATCH64_CTAS_PER_SM;
 
 // Largest co-resident grid of the persistent kernels on this device.
-int max_coop_grid_fp64(int device);
-int max_coop_grid_mixed(int device);
+// `served`: the server's instances (kServedCtasPerSm).
+int max_coop_grid_fp64(int device, bool served = false);
+int max_coop_grid_mixed(int device, bool served = false);
 // With a.sp.mean_row >= 0 the FP64 launch runs the mean-constraint variant
 // (its red holds kRedQMean quantities per CTA); the mixed form has none.
-cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s);
-cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s);
+cudaError_t launch_bicgstab64(const SolveArgs64& a, int grid, cudaStream_t s, bool served = false);
+cudaError_t launch_bicgstab_mixed(const SolveArgsMixed& a, int grid, cudaStream_t s, bool served = false);
 int max_coop_grid_mean(int device);
 int max_coop_grid_batch(int device, bool mixed);
 cudaError_t launch_bicgstab_batch(const BatchArgs& a, int grid, bool mixed, cudaStream_t s);

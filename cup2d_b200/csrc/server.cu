@@ -185,7 +185,7 @@ int cup2d_server::assemble(Mesh& m, std::unique_lock<std::mutex>& lk, cudaStream
   resident_bytes += need;  // reserved while assembling
   lk.unlock();
   const Clock::time_point t_asm = Clock::now();
-  int st = handle_create(&f, &o, stream, &h);
+  int st = handle_create(&f, &o, stream, true, &h);
   if (st == CUP2D_OK) st = cup2d_poisson_set_grid(h, team);
   double* db = nullptr;
   double* dx = nullptr;
@@ -466,8 +466,8 @@ int cup2d_server_create(const cup2d_server_opts* opts, cup2d_server** out) {
       return CUP2D_CUDA_ERROR;
     }
   }
-  const int grid_max = o.solve.precision == CUP2D_PREC_MIXED ? max_coop_grid_mixed(S->device)
-                                                              : max_coop_grid_fp64(S->device);
+  const int grid_max = o.solve.precision == CUP2D_PREC_MIXED ? max_coop_grid_mixed(S->device, true)
+                                                              : max_coop_grid_fp64(S->device, true);
   if (grid_max <= 0) {
     cup2d_server_destroy(S);
     return CUP2D_CUDA_ERROR;
