@@ -126,7 +126,7 @@ struct Fld {
 
 // Ghost of a fine cell (value vclose, next inward cell vfar) from coarse cell
 // (xc, yc) of block bc: ExpAMRSolver::interpolate on values.
-__device__ double interp_ghost(const Fld& w, int c, int64_t bc, int xc, int yc, double vclose, double vfar, double sT,
+__device__ __noinline__ double interp_ghost(const Fld& w, int c, int64_t bc, int xc, int yc, double vclose, double vfar, double sT,
                                bool xface) {
   const int t = xface ? yc : xc;
   auto cv = [&](int d) { return xface ? w.v(cidx(bc, xc, yc + d), c) : w.v(cidx(bc, xc + d, yc), c); };
