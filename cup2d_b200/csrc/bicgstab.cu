@@ -323,6 +323,20 @@ __device__ __forceinline__ double hsum_part(const MeshView& M, const T* __restri
 
 __device__ __forceinline__ bool owns_row(int row, int b0, int b1) { return row >= b0 * kBLEN && row < b1 * kBLEN; }
 
+// Whether this CTA's SpMV computes row `row`: a cell on a coarse/fine face
+// (its block's explicit mask bit set; possible for the corner cell across a
+// periodic edge) is an explicit row, computed by the CTA whose row range
+// [r0, r1) holds it; any other cell by the owner of its block.
+__device__ __forceinline__ bool computes_row(const MeshView& M, int row, int b0, int b1, int r0, int r1) {
+  const int blk = row / kBLEN, c = row % kBLEN;
+  const unsigned long long m = __ldg(M.xmask + blk);
+  if ((m >> c) & 1ull) {
+    const int xr = __ldg(M.xbase + blk) + __popcll(m & ((1ull << c) - 1ull));
+    return xr >= r0 && xr < r1;
+  }
+  return owns_row(row, b0, b1);
+}
+
 struct IterState {
   double rho, nr, nrh;  // (rhat,r), |r|^2, |rhat|^2 of the current residual
   double err_init;      // L-inf norm the relative test divides by
@@ -489,6 +503,9 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const Lane<T> L(lane);
   const double eps = 1e-21;
+  // MC: the CTA whose SpMV computes the mean row records that row's own
+  // product (its partials subtract it and add the sum h^2 v in its place)
+  const bool rec_mean = MC && computes_row(M, sp.mean_row, b0, b1, r0, r1);
   double rho_prev = 1.0, alpha = 1.0, omega = 1.0, beta;
   bool zero_pnu = true;
   double rho = st.rho, nr = st.nr, nrh = st.nrh;
@@ -562,7 +579,7 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
         // the mean row's own product and rhat, to swap in sum h^2 z below
         double v[4] = {epi.acc, hsum_part(M, V.z, b0, b1), 0.0, 0.0};
         __syncthreads();
-        if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) {
+        if (threadIdx.x == 0 && rec_mean) {
           const T y = __ldcg(V.nu + sp.mean_row), rv = __ldcg(V.rh + sp.mean_row);
           v[2] = dprod(rv, y);
           v[3] = (double)rv;
@@ -629,7 +646,7 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
       if constexpr (MC) {
         double v[6] = {epi.ts, epi.tt, hsum_part(M, V.z2, b0, b1), 0.0, 0.0, 0.0};
         __syncthreads();
-        if (threadIdx.x == 0 && owns_row(sp.mean_row, b0, b1)) {
+        if (threadIdx.x == 0 && rec_mean) {
           const T y = __ldcg(V.t + sp.mean_row), sv = __ldcg(V.r + sp.mean_row);
           v[3] = dprod(y, sv);
           v[4] = dprod(y, y);
