@@ -42,7 +42,8 @@
 // the Neumann compatibility condition); by default the recurrences restart
 // from it (rhat = r, p = nu = 0), which FP32 needs here: on the large
 // meshes the unrestarted FP32 recurrences diverge.  Convergence is declared
-// only on the true FP64 residual.
+// only on the true FP64 residual, and the best iterate (returned when the
+// solve stops unconverged) is the refreshed x with the lowest true residual.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -340,7 +341,7 @@ __device__ __forceinline__ bool computes_row(const MeshView& M, int row, int b0,
 struct IterState {
   double rho, nr, nrh;  // (rhat,r), |r|^2, |rhat|^2 of the current residual
   double err_init;      // L-inf norm the relative test divides by
-  double err_opt;       // best residual norm seen (recursive)
+  double err_opt;       // best residual norm seen (FP64: recursive; mixed: true)
   double err_true;      // mixed: last true residual |b - A x|_inf
   int restarts;
   int iters;
@@ -744,7 +745,7 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
         error = sm.gres[4];
         rmax_since = sqrt(nr);
         if ((st.err_true <= mx.tol_abs) || (st.err_true / st.err_init <= mx.tol_rel)) {
-          st.err_opt = fmin(st.err_opt, error);
+          st.err_opt = fmin(st.err_opt, st.err_true);
           st.best_is_x = true;
           st.status = CUP2D_OK;
           ++k;
@@ -753,10 +754,18 @@ __device__ bool bicgstab_loop(Smem<T>& sm, GridBarrier& B, const Pinv<T>& pin, c
       }
     }
     // convergence (BiCGSTAB.cu:571-600)
-    if (error < st.err_opt) {
+    if constexpr (RU) {
+      // mixed: an iterate is judged by its true residual, which only a
+      // refresh computes (err_opt is the best true residual so far).  x
+      // moves in every pass E, so between refreshes the best iterate is the
+      // copy in xo, written by the pass E after the refresh that found it:
+      // one copy per refresh, not one per iteration
+      st.best_is_x = refreshed && st.err_true < st.err_opt;
+      if (st.best_is_x) st.err_opt = st.err_true;
+    } else if (error < st.err_opt) {
       st.err_opt = error;
       st.best_is_x = true;
-      if (!RU && ((error <= sp.tol_abs) || (error / st.err_init <= sp.tol_rel))) {
+      if ((error <= sp.tol_abs) || (error / st.err_init <= sp.tol_rel)) {
         st.status = CUP2D_OK;
         ++k;
         break;
@@ -948,7 +957,7 @@ __device__ bool solve_mixed(Smem<float>& sm, GridBarrier& B, const Pinv<float>& 
   IterState st;
   st.err_init = sm.gres[0];
   st.err_true = sm.gres[0];
-  st.err_opt = sm.gres[4];
+  st.err_opt = sm.gres[0];  // best true residual: x0's
   st.rho = sm.gres[1];
   st.nr = sm.gres[2];
   st.nrh = sm.gres[3];

@@ -101,7 +101,9 @@ typedef struct cup2d_solve_stats {
   int32_t refinements;     /* mixed: FP64 true-residual replacements taken */
   double err_init;         /* |b - A x0|_inf */
   double err_final;        /* fp64: best recursive |r|_inf (the reference's test);
-                              mixed: final true |b - A x|_inf in FP64 */
+                              mixed: true |b - A x|_inf in FP64 of the returned
+                              x (converged: the final iterate; otherwise the
+                              refreshed iterate with the lowest one) */
   double rel_res_inf;      /* err_final / err_init */
   double solve_ms;         /* device time of the solve (CUDA events) */
 } cup2d_solve_stats;

@@ -185,6 +185,23 @@ def test_mixed_solve_matches_oracle(cuda):
     assert _rel_l2(x, x_o) <= 1e-6
 
 
+def test_mixed_unconverged_returns_best_refreshed_iterate(cuda):
+    """Mixed form stopped by the iteration cap: the returned x is a refreshed
+    iterate, and err_final is its true residual |(b - mean b) - A x|_inf,
+    the lowest of the refreshes (no later refresh is reported lower)."""
+    m = MESHES["sized_1500"]
+    b = m.rhs_fourier(4)
+    A = oracle.Matrix(m)
+    with Solver(m, tol_rel=1e-12, max_iter=150, precision="mixed") as s:
+        x = s.solve(b)
+        st = s.last_stats
+    assert st["status"] == L.NOT_CONVERGED and st["iterations"] == 150, st
+    assert st["refinements"] >= 2
+    r = (b - b.mean()) - A.spmv(x)
+    assert np.max(np.abs(r)) == pytest.approx(st["err_final"], rel=1e-9)
+    assert st["err_final"] < st["err_init"]
+
+
 def test_not_converged_and_breakdown_status(cuda):
     m = MESHES["small"]
     b = m.rhs_fourier(1)
