@@ -38,6 +38,39 @@ __device__ __forceinline__ unsigned long long explicit_mask(const MeshView& M, i
   return 0ull;
 }
 
+// Entries of an explicit row whose loads are issued as one batch: 8 in FP32,
+// 4 in FP64 (whose batch kernels run at 80 registers a thread).
+template <class T>
+constexpr int kRowBatch = sizeof(T) == 4 ? 8 : 4;
+
+// sum_k vals[k] z[xcol[k]] of an explicit row, k ascending over [k0, k1).
+// The columns and values of the first kRowBatch entries are requested
+// together, then their gathers together (two dependent round trips for a
+// row of up to kRowBatch entries; coarse/fine rows hold 7-8); the rest of a
+// longer row follows in a plain loop.  The sum is accumulated in k order, as the
+// assembled row is.
+template <class T>
+__device__ __forceinline__ T explicit_row(const MeshView& M, const T* __restrict__ z, int k0, int k1) {
+  constexpr int W = kRowBatch<T>;
+  const T* __restrict__ vals = row_vals<T>(M);
+  int col[W];
+  T v[W], g[W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const bool in = k0 + j < k1;
+    col[j] = in ? __ldg(M.xcol + k0 + j) : 0;
+    v[j] = in ? __ldg(vals + k0 + j) : T(0);
+  }
+#pragma unroll
+  for (int j = 0; j < W; ++j) g[j] = k0 + j < k1 ? ldcg(z + col[j]) : T(0);
+  T acc = T(0);
+#pragma unroll
+  for (int j = 0; j < W; ++j)
+    if (k0 + j < k1) acc += v[j] * g[j];
+  for (int k = k0 + W; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
+  return acc;
+}
+
 // ------------------------------------------------ 16-byte lane layout ----
 //
 // The range passes move 16 bytes per lane and access: V = 4 consecutive
@@ -259,18 +292,19 @@ __device__ __forceinline__ void spmv_range(const MeshView& M, const T* __restric
     chunk_epilogue<T>(M, ga, L, ba, va, pa, epi, row);
   }
   for (; r < r1; r += blockDim.x) {
-    const Pre pre = epi.load1(cell);
-    const T* __restrict__ vals = row_vals<T>(M);
-    T acc = T(0);
-#pragma unroll 4
-    for (int k = k0; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
-    epi.one(cell, acc, pre, 0);
+    // the next row's offsets are requested before this row's gathers
     const int rn = r + blockDim.x;
+    int k0n = 0, k1n = 0, celln = 0;
     if (rn < r1) {
-      k0 = __ldg(M.xptr + rn);
-      k1 = __ldg(M.xptr + rn + 1);
-      cell = __ldg(M.rowcell + rn);
+      k0n = __ldg(M.xptr + rn);
+      k1n = __ldg(M.xptr + rn + 1);
+      celln = __ldg(M.rowcell + rn);
     }
+    const Pre pre = epi.load1(cell);
+    epi.one(cell, explicit_row<T>(M, z, k0, k1), pre, 0);
+    k0 = k0n;
+    k1 = k1n;
+    cell = celln;
   }
 }
 
@@ -373,18 +407,19 @@ __device__ __forceinline__ void spmv_range_staged(const MeshView& M, const T* __
   // the explicit rows while the first chunks' copies are in flight: their
   // dependent loads (offsets, columns, gathered z) overlap the copies
   for (; r < r1; r += blockDim.x) {
-    const Pre pre = epi.load1(cell);
-    const T* __restrict__ vals = row_vals<T>(M);
-    T acc = T(0);
-#pragma unroll 4
-    for (int k = k0; k < k1; ++k) acc += __ldg(vals + k) * ldcg(z + __ldg(M.xcol + k));
-    epi.one(cell, acc, pre, 0);
+    // the next row's offsets are requested before this row's gathers
     const int rn = r + blockDim.x;
+    int k0n = 0, k1n = 0, celln = 0;
     if (rn < r1) {
-      k0 = __ldg(M.xptr + rn);
-      k1 = __ldg(M.xptr + rn + 1);
-      cell = __ldg(M.rowcell + rn);
+      k0n = __ldg(M.xptr + rn);
+      k1n = __ldg(M.xptr + rn + 1);
+      celln = __ldg(M.rowcell + rn);
     }
+    const Pre pre = epi.load1(cell);
+    epi.one(cell, explicit_row<T>(M, z, k0, k1), pre, 0);
+    k0 = k0n;
+    k1 = k1n;
+    cell = celln;
   }
   for (int k = 0; k < K; ++k) {
     cp_async_wait_n<S - 2>();  // this lane's copies of chunk k have landed
