@@ -1064,7 +1064,7 @@ def main(argv=None) -> int:
     ap.add_argument("--tune-iters", type=int, default=0,
                     help="batch autotuner: iterations per problem of a candidate (0 = full solves: a fixed "
                          "iteration count ignores the tail of the largest problems and favours small teams)")
-    ap.add_argument("--tune-teams", default="6,8,12,16", help="batch autotuner: candidate teams")
+    ap.add_argument("--tune-teams", default="5,6,8,12", help="batch autotuner: candidate teams")
     ap.add_argument("--tune-cps", default="0", help="batch autotuner: candidate CTAs per SM (0 = all)")
     ap.add_argument("--no-spmv", action="store_true", help="batch: skip the standalone SpMV leg")
     ap.add_argument("--spmv-only", action="store_true", help="the standalone SpMV leg alone (profiling runs)")

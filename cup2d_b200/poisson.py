@@ -381,7 +381,7 @@ class BatchSolver:
         """CTAs per SM of batched launches (0 = as many as fit)."""
         L.check(L.lib().cup2d_batch_set_occupancy(self._h, int(ctas_per_sm)), "cup2d_batch_set_occupancy")
 
-    def autotune(self, bs, xs, teams=(6, 8, 12, 16), ctas_per_sm=(0,), iters: int = 0,
+    def autotune(self, bs, xs, teams=(5, 6, 8, 12), ctas_per_sm=(0,), iters: int = 0,
                  cache: Optional[str] = None) -> tuple[int, int]:
         """Picks the launch shape for this batch -- team size (CTAs per
         problem) and occupancy cap (CTAs per SM, 0 = all that fit): every
