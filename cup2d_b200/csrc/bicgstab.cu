@@ -81,10 +81,12 @@ static_assert(Q_MX + 1 <= kRedQMean, "reduction slots (mean constraint)");
 
 // Shared memory of the solve kernels, per precision T of the Krylov vectors:
 // P^-1, the P^-1 staging tiles, the staged SpMV rings and the reduction
-// scratch.  Both layouts stay below 54 KB so that three CTAs per SM fit the
-// 164 KB shared carve-out and leave 92 KB of the unified L1/shared array as
-// L1 (the kernels' spill reloads and table reads live there: the same
-// kernel with the whole array given to shared memory ran 11 % slower).
+// scratch.  Both layouts stay below 54 KB so that the kernels run at 3 CTAs
+// per SM (the FP64 batch and the server's instances) within the 164 KB
+// shared carve-out and leave 92 KB of the unified L1/shared array as L1
+// (their spill reloads and table reads live there: the same kernel with the
+// whole array given to shared memory ran 11 % slower).  The kernels at 2
+// CTAs per SM take a smaller carve-out and keep more L1.
 template <class T>
 union TileSmem;
 template <>
