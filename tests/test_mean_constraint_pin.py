@@ -113,3 +113,26 @@ def test_oracle_mean_iteration_cap_like_reference(case):
     # from 3e-8 to 1.6e-3 with the OpenMP thread count, i.e. summation order)
     for rel in (float(fx["err_opt"]), st["err_opt"] / st["err_init"]):
         assert 1e-8 < rel < 0.1
+
+
+def _on_coarse_fine_face(m, row):
+    """Whether the row couples cells of another level (an explicit row of
+    the device assembly, computed by whichever CTA holds it in the row
+    partition, not necessarily the owner of its block)."""
+    rp, col, _ = oracle.Matrix(m).csr()
+    cols = col[rp[row]:rp[row + 1]]
+    return bool(np.any(m.level[cols // 64] != m.level[row // 64]))
+
+
+def test_mean_row_cases_cover_explicit_and_stencil_rows():
+    """The constrained reference cases include a mean row on a coarse/fine
+    face (the corner cell across a periodic edge of periodic_xy_rev) and
+    mean rows inside the stencil, so the GPU tests of those cases cover
+    both ways the solver records the mean row's own product."""
+    kinds = {}
+    for case in F.MEAN_CASES:
+        m, _ = F.mean_case_rhs(case)
+        kinds[case] = _on_coarse_fine_face(m, oracle.mean_row(m))
+    assert kinds["mean_periodic_xy_rev"]
+    assert not kinds["mean_small"] and not kinds["mean_sized_1500_rev"]
+
