@@ -940,9 +940,70 @@ def run_reference_batch(args) -> dict:
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_reference_gpu_batch(args) -> dict:
+    """The reference's own GPU path on the batched workload, for comparison
+    (`--impl reference --ref-gpu`; the reference arm's line stays the CPU
+    one): CUP2D's ExpAMRSolver::solve with its cuBLAS/cuSPARSE BiCGSTAB
+    (source/Poisson/BiCGSTAB.cu:412-620), its Poisson sources compiled
+    unchanged against one-rank stand-ins (oracle/_ref), one problem per call
+    as CUP2D runs it, on the slices the CPU arm solves.  A call constructs
+    the solver (P^-1, library handles, device buffers), assembles on the
+    host (getMat), copies b and x in, solves with the reference's hard-coded
+    1000-iteration cap and copies x back; wall clock per step.  The same
+    calls with tol_rel = 1 (one iteration) measure the fixed part of a call,
+    reported beside it ("per_call_fixed_ms", "solve_only")."""
+    import oracle.ref as R
+    from cup2d_b200.problems import batch_problems
+    if not R.available("gpu"):
+        return {"impl": "reference", "unavailable": "the reference GPU checker (oracle/_ref) is not built"}
+    meshes = batch_problems(args.batch, seed=3)
+    seeds = [100 + i for i in range(len(meshes))]
+    parts = cpu_slices(meshes)
+    times, fixed, its = [], [], []
+    solves = capped = cells = 0
+    for k in range(args.warmup + args.steps):
+        idx = parts[k % len(parts)]
+        bs = [meshes[i].rhs_fourier(seeds[i]) for i in idx]
+        t0 = time.perf_counter()
+        sts = [R.solve(meshes[i], b, tol_rel=TOL)[1] for i, b in zip(idx, bs)]
+        dt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for i, b in zip(idx, bs):
+            R.solve(meshes[i], b, tol_rel=1.0)
+        df = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+            fixed.append(df)
+            solves += len(idx)
+            cells += sum(meshes[i].ncells for i in idx)
+            capped += sum(1 for s in sts if not s["converged"])
+            its += [s["iterations"] for s in sts if s["iterations"] is not None]
+    tot, tfix = sum(times), sum(fixed)
+    v = solves / tot
+    sample = (f"step k: slice k mod {len(parts)} of the batch ({len(parts[0])} problems, one of each size stratum), "
+              f"x0 = 0 to rel. 1e-6, one ExpAMRSolver per call (construction, host getMat, GPU BiCGSTAB with the "
+              f"reference's 1000-iteration cap: {capped} of {solves} capped), {solves} solves in {tot:.1f} s")
+    steps = len(times)
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded Fourier-velocity divergence RHS on disk-refined AMR forests)",
+            "impl": "reference", "path": "reference GPU: ExpAMRSolver::solve, cuBLAS/cuSPARSE BiCGSTAB (oracle/_ref)",
+            "config": {"workload": batch_label(meshes, 0),
+                       "tol": "true |b-Ax|_inf / |b|_inf <= 1e-6, x0 = 0 (every problem)"},
+            "iterations_mean": statistics.mean(its) if its else None, "capped": capped,
+            "per_call_fixed_ms": tfix / solves * 1e3,
+            "solve_only": {"value": solves / max(tot - tfix, 1e-9), "unit": UNIT,
+                           "how": "steps' time less the same calls at tol_rel = 1"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": int(16 * cells / steps),
+                    "d2h_bytes_per_step": int(8 * cells / steps)}}
+
+
 def run_reference(args, world, rank) -> dict | None:
     if rank != 0:
         return None
+    if args.workload == "batch" and args.ref_gpu:
+        return run_reference_gpu_batch(args)
     if args.workload == "batch":
         return run_reference_batch(args)
     import oracle
@@ -1055,6 +1116,9 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="with --impl reference, batch: time the reference's own GPU path (oracle/_ref) instead "
+                         "of the CPU reference algorithm")
     ap.add_argument("--workload", choices=["batch", "large", "small", "serve", "timestep"], default="batch")
     ap.add_argument("--ts-steps", type=int, default=500, help="timestep workload: time steps per leg")
     ap.add_argument("--batch", type=int, default=512, help="batch workload: number of problems")
