@@ -105,12 +105,21 @@ def test_oracle_mean_iteration_cap_like_reference(case):
     best residual far from the tolerance (the printed figure is relative)."""
     fx = load_solve_fixture(case)
     m, b = F.mean_case_rhs(case)
-    x, st = oracle.solve(m, b, tol_rel=1e-8, max_iter=1000, mean_constraint=True)
+    # two OpenMP threads: a reduction adds its per-thread partials in the
+    # order the threads arrive, so with three or more the oracle's sums, and
+    # where this chaotic solve stops, differ from run to run; two partials
+    # sum the same either way
+    threads = oracle.num_threads()
+    oracle.set_threads(2)
+    try:
+        x, st = oracle.solve(m, b, tol_rel=1e-8, max_iter=1000, mean_constraint=True)
+    finally:
+        oracle.set_threads(threads)
     assert int(fx["iterations"]) == 1000 and st["iterations"] == 1000 and not st["converged"]
     assert st["err_init"] == pytest.approx(float(fx["err_init"]), rel=1e-5)
     assert int(fx["restarts"]) >= 5 and st["restarts"] >= 5
     # where it stops is chaotic (the oracle's best residual at the cap moves
-    # from 3e-8 to 1.6e-3 with the OpenMP thread count, i.e. summation order)
+    # from 1e-7 to 9e-3 with the summation order, i.e. the OpenMP threads)
     for rel in (float(fx["err_opt"]), st["err_opt"] / st["err_init"]):
         assert 1e-8 < rel < 0.1
 
