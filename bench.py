@@ -1002,7 +1002,7 @@ def run_reference_gpu_batch(args) -> dict:
 def run_reference(args, world, rank) -> dict | None:
     if rank != 0:
         return None
-    if args.workload == "batch" and args.ref_gpu:
+    if args.workload == "batch" and getattr(args, "ref_gpu", False):
         return run_reference_gpu_batch(args)
     if args.workload == "batch":
         return run_reference_batch(args)
